@@ -1,0 +1,266 @@
+/*
+ * mmb200 — B200 (sm_100a) implementation of MicroMagnum's effective-field + LLG + Runge-Kutta
+ * hot path, behind a C ABI.
+ *
+ * Conventions shared by every entry point
+ *  - Grids are nx*ny*nz cells, linear index i = z*nx*ny + y*nx + x (x fastest), the layout of
+ *    the reference's Matrix/VectorMatrix (src/magneto/mmm/exchange/exchange_cpu.cpp:81).
+ *  - A vector field is structure-of-arrays: three arrays of N = nx*ny*nz elements back to back
+ *    (x components, then y, then z), like the reference's VectorMatrix (matrix/matrix/vector/
+ *    VectorMatrix.h:35-79).  Units are the reference's: M and H in A/m, times in seconds.
+ *  - All array arguments are DEVICE pointers unless the parameter name ends in `_host`.
+ *  - `prec` selects the element type of every array argument of a call: MM_F64 -> double,
+ *    MM_F32 -> float.  MM_F64 is the plain mode (the reference's `-G`, CUDA_64), MM_F32 the
+ *    single-precision mode (`-g`, CUDA_32).
+ *  - `stream` is a cudaStream_t (NULL = legacy default stream).  Calls that return a scalar to
+ *    the host synchronise that stream; all others are stream-ordered and return immediately.
+ *  - No entry point throws.  Each returns an mm_status; on failure mm_last_error() returns a
+ *    message for the calling thread.  The library never falls back to a CPU implementation.
+ */
+#ifndef MMB200_H
+#define MMB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MM_API __attribute__((visibility("default")))
+#define MM_ABI_VERSION 1
+
+typedef enum {
+	MM_OK = 0,
+	MM_ERR_INVALID_ARGUMENT = 1,  /* bad sizes, null pointers, unknown enum value */
+	MM_ERR_CUDA = 2,              /* a CUDA runtime call or kernel launch failed */
+	MM_ERR_OUT_OF_MEMORY = 3,     /* device allocation failed */
+	MM_ERR_UNSUPPORTED = 4,       /* valid request the library does not implement */
+	MM_ERR_NOT_FINITE = 5,        /* NaN/Inf detected in a solver state */
+	MM_ERR_TIMEOUT = 6            /* a bounded device-side wait gave up */
+} mm_status;
+
+typedef enum { MM_F64 = 0, MM_F32 = 1 } mm_precision;
+
+/* Padding strategies of the demag tensor (src/magneto/mmm/demag/tensor_round.h; same values as
+ * the reference's PADDING_* enum exported at bindings/mmm/demag.i:27-42). */
+typedef enum {
+	MM_PADDING_DISABLE = 0,
+	MM_PADDING_ROUND_2 = 1,
+	MM_PADDING_ROUND_4 = 2,
+	MM_PADDING_ROUND_8 = 3,
+	MM_PADDING_ROUND_POT = 4,
+	MM_PADDING_SMALL_PRIME_FACTORS = 5
+} mm_padding;
+
+/* Message describing the last failure on the calling thread ("" if none). */
+MM_API const char *mm_last_error(void);
+MM_API int mm_abi_version(void);
+/* Number of kernels this library has launched in the process (for launch accounting). */
+MM_API uint64_t mm_kernel_launch_count(void);
+
+/* ---------------------------------------------------------------------------------------------
+ * Field terms: one call per term, same arguments and results as the reference's magneto calls.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Exchange field, 6-neighbour stencil, Neumann boundaries, neighbours with Ms == 0 skipped,
+ * optional periodic boundaries.  Replaces magneto.exchange (bindings/mmm/exchange.i:24-39 ->
+ * mmm/exchange/exchange.cpp:31-58).  If energy_host is non-NULL, *energy_host receives
+ * -mu0/2 * dx*dy*dz * sum_i M_i.H_i (the CUDA path's return value, exchange_cuda.cu:456). */
+MM_API mm_status mm_exchange(int prec, int nx, int ny, int nz, double dx, double dy, double dz,
+                             int pbc_x, int pbc_y, int pbc_z, const void *Ms, const void *A,
+                             const void *M, void *H, double *energy_host, void *stream);
+
+/* Uniaxial anisotropy H = 2 k (m.a) a / (mu0 Ms), zero where Ms == 0 or k == 0.  Replaces
+ * magneto.uniaxial_anisotropy (bindings/mmm/anisotropy.i:24-31 -> mmm/anisotropy/
+ * anisotropy.cpp:33-58).  energy_host (optional) receives sum_i k_i |a_i x m_i|^2, the CPU
+ * path's return value (anisotropy_cpu.cpp:64-68). */
+MM_API mm_status mm_uniaxial_anisotropy(int prec, size_t n, const void *axis, const void *k,
+                                        const void *Ms, const void *M, void *H,
+                                        double *energy_host, void *stream);
+
+/* Cubic anisotropy (axis3 = axis1 x axis2).  Replaces magneto.cubic_anisotropy
+ * (anisotropy.i:32-39 -> anisotropy.cpp:60-88).  energy_host (optional) receives
+ * sum_i k_i (a1^2 a2^2 + a1^2 a3^2 + a2^2 a3^2). */
+MM_API mm_status mm_cubic_anisotropy(int prec, size_t n, const void *axis1, const void *axis2,
+                                     const void *k, const void *Ms, const void *M, void *H,
+                                     double *energy_host, void *stream);
+
+/* LLG right-hand side dM = f1 M x H + f2 M x (M x H).  Replaces magneto.llge
+ * (bindings/mmm/llge.i:24-29 -> mmm/llge/llge.cpp:33-59). */
+MM_API mm_status mm_llge(int prec, size_t n, const void *f1, const void *f2, const void *M,
+                         const void *H, void *dM, void *stream);
+
+/* Zhang-Li spin-transfer torque, finite differences of M (one-sided at the edges, zero along a
+ * dimension of size 1).  Replaces magneto.fdm_zhangli (bindings/mmm/zhangli.i:24-32 ->
+ * mmm/spintorque/fdm_zhangli.cpp:33-53). */
+MM_API mm_status mm_fdm_zhangli(int prec, int nx, int ny, int nz, double dx, double dy,
+                                double dz, int do_precess, const void *P, const void *xi,
+                                const void *Ms, const void *alpha, const void *j,
+                                const void *M, void *dM, void *stream);
+
+/* max_i |M_i| / scale_i over cells with scale_i != 0.  Replaces magneto.scaled_abs_max
+ * (bindings/math.i:66 -> math/ScaledAbsMax.cpp:52-68).  Synchronises `stream`. */
+MM_API mm_status mm_scaled_abs_max(int prec, size_t n, const void *M, const void *scale,
+                                   double *result_host, void *stream);
+
+/* M_i <- Ms_i M_i / |M_i| (0 where |M_i| == 0).  Replaces VectorMatrix::normalize(Matrix)
+ * (matrix/matrix/vector/VectorMatrix.cpp:218-230) as called by the solver after every accepted
+ * step (magnum/micromagnetics/micro_magnetics.py:49-50). */
+MM_API mm_status mm_normalize(int prec, size_t n, const void *Ms, void *M, void *stream);
+
+/* Runge-Kutta stage state ytmp = y + h * sum_{j<step} b[step][j] k_j and the final combination
+ * y += h sum c_j k_j, y_error = h sum ec_j k_j, for any explicit tableau with up to 8 stages.
+ * `b` is the row b[step][0..step-1]; k is an array of `nk` device pointers (host array).
+ * Replaces magneto.rk_prepare_step / rk_combine_result (bindings/evolver.i:63-92 ->
+ * evolver/runge_kutta.cpp:32-96). */
+MM_API mm_status mm_rk_prepare_step(int prec, size_t n, int step, double h, const double *b_host,
+                                    const void *const *k_host, const void *y, void *ytmp,
+                                    void *stream);
+MM_API mm_status mm_rk_combine_result(int prec, size_t n, int nk, double h, const double *c_host,
+                                      const double *ec_host, const void *const *k_host, void *y,
+                                      void *y_error, void *stream);
+
+/* ---------------------------------------------------------------------------------------------
+ * Demagnetisation: tensor and zero-padded FFT convolution.
+ * ------------------------------------------------------------------------------------------- */
+
+/* Padded FFT length of one dimension: the reference's round_tensor_dimension
+ * (mmm/demag/tensor_round.cpp:90-106). */
+MM_API int mm_round_tensor_dimension(int dim, int periodic, int padding);
+
+/* Newell demagnetisation tensor, already negated (H = N * M), computed on the GPU in FP64 into
+ * N_out (device, 6*ex*ey*ez doubles, component index fastest then x, y, z: the reference's
+ * Matrix(Shape(6, ex, ey, ez)) layout, mmm/demag/tensor.cpp:41,167-180).  ex/ey/ez are the
+ * padded sizes (mm_round_tensor_dimension).  Replaces magneto.GenerateDemagTensor
+ * (bindings/mmm/demag.i:27-42 -> mmm/demag/demag_tensor.cpp:116-186).  Periodic boundaries
+ * return MM_ERR_UNSUPPORTED; a tensor computed elsewhere can still be passed to
+ * mm_conv_create. */
+MM_API mm_status mm_demag_tensor(int nx, int ny, int nz, double dx, double dy, double dz,
+                                 int ex, int ey, int ez, double *N_out, void *stream);
+
+/* Zero-padded FFT convolution H = N * M with a symmetric tensor field.  Replaces
+ * magneto.SymmetricMatrixVectorConvolution_FFT (bindings/math.i:27-33 ->
+ * math/conv/SymmetricMatrixVectorConvolution_FFT.cpp:31-65, MatrixVectorConvolution_FFT.cpp:
+ * 110-375).  N_device is the tensor in the layout of mm_demag_tensor (FP64); the plan keeps its
+ * spectrum in working precision `prec` and owns its scratch.  execute() takes M and writes H in
+ * `prec`. */
+typedef struct mm_conv mm_conv;
+MM_API mm_status mm_conv_create(mm_conv **out, int prec, int nx, int ny, int nz, int ex, int ey,
+                                int ez, const double *N_device, void *stream);
+MM_API mm_status mm_conv_execute(mm_conv *conv, const void *M, void *H, void *stream);
+MM_API mm_status mm_conv_destroy(mm_conv *conv);
+
+/* ---------------------------------------------------------------------------------------------
+ * Solver: the fused B200 path.  State, stage vectors, demag spectra and the step controller live
+ * on the device; one call advances the state by whole Runge-Kutta steps with the reference's
+ * semantics (magnum/evolver/runge_kutta.py:47-137 with MicroMagneticsStepSizeController,
+ * magnum/micromagnetics/micro_magnetics_stepsize_controller.py:35-73).
+ * ------------------------------------------------------------------------------------------- */
+
+/* Per-region material.  Every cell carries a region index (uint8) into a table of these. */
+typedef struct {
+	double Ms;             /* saturation magnetisation [A/m]; 0 marks empty cells */
+	double A;              /* exchange stiffness [J/m] */
+	double alpha;          /* Gilbert damping */
+	double k_uniaxial;     /* uniaxial anisotropy constant [J/m^3] */
+	double k_cubic;        /* cubic anisotropy constant [J/m^3] */
+	double axis1[3];       /* uniaxial axis / first cubic axis */
+	double axis2[3];       /* second cubic axis */
+	double P;              /* spin polarisation (Zhang-Li) */
+	double xi;             /* non-adiabaticity (Zhang-Li) */
+	double j[3];           /* current density [A/m^2] (Zhang-Li) */
+} mm_material;
+
+typedef enum {
+	MM_RK_RKF45 = 0, MM_RK_CC45 = 1, MM_RK_DP54 = 2, MM_RK_RK23 = 3
+} mm_tableau;
+
+enum {
+	MM_TERM_DEMAG = 1, MM_TERM_EXCHANGE = 2, MM_TERM_UNIAXIAL = 4, MM_TERM_CUBIC = 8,
+	MM_TERM_ZHANGLI = 16, MM_TERM_ZEEMAN = 32
+};
+
+typedef struct {
+	int nx, ny, nz;
+	double dx, dy, dz;
+	int precision;          /* mm_precision */
+	int tableau;            /* mm_tableau */
+	int terms;              /* MM_TERM_* bit set */
+	int do_precess;         /* LLG precession term (LandauLifshitzGilbert(do_precess)) */
+	int zl_do_precess;      /* Zhang-Li precession variant (SpinTorque(do_precess)) */
+	int padding;            /* mm_padding for the demag tensor */
+	double eps_abs, eps_rel;/* MicroMagneticsStepSizeController tolerances */
+	double h0;              /* first step size tried (MicroMagnetics.createState: 1e-13) */
+	/* Uniform applied field H(t) = H_ext + H_pulse * min(t / pulse_rise, 1) [A/m];
+	 * pulse_rise <= 0 means a static H_ext + H_pulse. */
+	double H_ext[3];
+	double H_pulse[3];
+	double pulse_rise;
+	/* 1 (default semantics of the reference): after a rejected step the next attempt reuses the
+	 * rejected attempt's last stage as its first (runge_kutta.py:67-70,99-100,131-134).
+	 * 0: re-evaluate the first stage after a rejection. */
+	int fsal_reuse_after_reject;
+} mm_solver_config;
+
+typedef struct {
+	double t;              /* simulation time [s] */
+	double h;              /* last accepted step size */
+	double h_next;         /* step size the next attempt will try */
+	int64_t steps;         /* accepted steps */
+	int64_t attempts;      /* attempts including rejected ones */
+	int64_t rejected;      /* rejected attempts */
+	double last_error;     /* e_abs of the last attempt (max |m_err|) */
+	double last_max_dmdt;  /* max |dm/dt| of the last attempt [rad/s] */
+	int not_finite;        /* 1 if a NaN/Inf was seen in the last attempt */
+} mm_solver_stats;
+
+typedef struct mm_solver mm_solver;
+
+/* regions_host: N region indices (NULL: every cell region 0); materials_host: num_materials
+ * entries (<= 256).  tensor_device: optional FP64 tensor in the mm_demag_tensor layout for the
+ * padded sizes of config->padding (NULL: generate it on the GPU). */
+MM_API mm_status mm_solver_create(mm_solver **out, const mm_solver_config *config,
+                                  int num_materials, const mm_material *materials_host,
+                                  const uint8_t *regions_host, const double *tensor_device,
+                                  void *stream);
+MM_API mm_status mm_solver_destroy(mm_solver *s);
+
+/* Set / read the magnetisation M [A/m] (FP64 device arrays, SoA).  set_M re-normalises to Ms
+ * like LandauLifshitzGilbert.update("M") (landau_lifshitz_gilbert.py:84-88), resets t and the
+ * step counters, and forgets the first-same-as-last stage. */
+MM_API mm_status mm_solver_set_M(mm_solver *s, const double *M_device, void *stream);
+MM_API mm_status mm_solver_get_M(mm_solver *s, double *M_device, void *stream);
+MM_API mm_status mm_solver_set_time(mm_solver *s, double t, double h_next, void *stream);
+
+/* One accepted step toward t_max: RungeKutta.evolve(state, t_max) (runge_kutta.py:47-87)
+ * followed by finish_step (normalisation).  Synchronises `stream`. */
+MM_API mm_status mm_solver_step(mm_solver *s, double t_max, void *stream);
+
+/* Advance until t >= t_end (condition.Time), clamping steps to every multiple of
+ * sample_dt (> 0; condition.EveryNthSecond) and writing <M> [A/m] at each such time into
+ * samples_host (3 doubles per sample, at most max_samples) with the time into
+ * sample_t_host.  *num_samples receives the count.  Pass sample_dt <= 0 for no sampling. */
+MM_API mm_status mm_solver_run(mm_solver *s, double t_end, double sample_dt,
+                               double *sample_t_host, double *samples_host, int max_samples,
+                               int *num_samples, void *stream);
+
+/* One Runge-Kutta attempt with step size h from the current state, with no state update
+ * (used for throughput measurement).  Stream-ordered; no host synchronisation. */
+MM_API mm_status mm_solver_attempt(mm_solver *s, double h, void *stream);
+
+/* Effective field H_eff [A/m] and dM/dt [A/(m s)] at the current state (FP64 device arrays,
+ * either may be NULL), with H_demag alone optionally into H_demag_device. */
+MM_API mm_status mm_solver_eval(mm_solver *s, double *H_eff_device, double *dMdt_device,
+                                double *H_demag_device, void *stream);
+
+MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *stream);
+
+/* <M> [A/m] averaged over all cells (VectorMatrix::average). Synchronises `stream`. */
+MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg_host3, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MMB200_H */

@@ -1,0 +1,135 @@
+"""ctypes binding of libmmb200.so, the C ABI declared in include/mmb200.h.
+
+The library is built in-tree (``micromagnum_b200/libmmb200.so``, see ``build()``).  Loading
+fails loudly when it is missing: there is no CPU implementation behind this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmmb200.so")
+
+MM_OK = 0
+STATUS_NAMES = {
+    0: "MM_OK", 1: "MM_ERR_INVALID_ARGUMENT", 2: "MM_ERR_CUDA", 3: "MM_ERR_OUT_OF_MEMORY",
+    4: "MM_ERR_UNSUPPORTED", 5: "MM_ERR_NOT_FINITE", 6: "MM_ERR_TIMEOUT",
+}
+MM_F64, MM_F32 = 0, 1
+MM_RK_RKF45, MM_RK_CC45, MM_RK_DP54, MM_RK_RK23 = 0, 1, 2, 3
+MM_TERM_DEMAG, MM_TERM_EXCHANGE, MM_TERM_UNIAXIAL = 1, 2, 4
+MM_TERM_CUBIC, MM_TERM_ZHANGLI, MM_TERM_ZEEMAN = 8, 16, 32
+
+
+class MMError(RuntimeError):
+    """A failed mmb200 call (the reference raises RuntimeError from its SWIG layer)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class mm_material(ctypes.Structure):
+    _fields_ = [
+        ("Ms", ctypes.c_double), ("A", ctypes.c_double), ("alpha", ctypes.c_double),
+        ("k_uniaxial", ctypes.c_double), ("k_cubic", ctypes.c_double),
+        ("axis1", ctypes.c_double * 3), ("axis2", ctypes.c_double * 3),
+        ("P", ctypes.c_double), ("xi", ctypes.c_double), ("j", ctypes.c_double * 3),
+    ]
+
+
+class mm_solver_config(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("precision", ctypes.c_int), ("tableau", ctypes.c_int), ("terms", ctypes.c_int),
+        ("do_precess", ctypes.c_int), ("zl_do_precess", ctypes.c_int), ("padding", ctypes.c_int),
+        ("eps_abs", ctypes.c_double), ("eps_rel", ctypes.c_double), ("h0", ctypes.c_double),
+        ("H_ext", ctypes.c_double * 3), ("H_pulse", ctypes.c_double * 3),
+        ("pulse_rise", ctypes.c_double), ("fsal_reuse_after_reject", ctypes.c_int),
+    ]
+
+
+class mm_solver_stats(ctypes.Structure):
+    _fields_ = [
+        ("t", ctypes.c_double), ("h", ctypes.c_double), ("h_next", ctypes.c_double),
+        ("steps", ctypes.c_int64), ("attempts", ctypes.c_int64), ("rejected", ctypes.c_int64),
+        ("last_error", ctypes.c_double), ("last_max_dmdt", ctypes.c_double),
+        ("not_finite", ctypes.c_int),
+    ]
+
+
+# (name, restype, argtypes) for every entry point of include/mmb200.h
+_VP, _D, _I, _SZ = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_size_t
+_DP = ctypes.POINTER(ctypes.c_double)
+_PROTOS = [
+    ("mm_last_error", ctypes.c_char_p, []),
+    ("mm_abi_version", _I, []),
+    ("mm_kernel_launch_count", ctypes.c_uint64, []),
+    ("mm_exchange", _I, [_I, _I, _I, _I, _D, _D, _D, _I, _I, _I, _VP, _VP, _VP, _VP, _DP, _VP]),
+    ("mm_uniaxial_anisotropy", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _DP, _VP]),
+    ("mm_cubic_anisotropy", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _VP, _DP, _VP]),
+    ("mm_llge", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("mm_fdm_zhangli", _I, [_I, _I, _I, _I, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
+    ("mm_scaled_abs_max", _I, [_I, _SZ, _VP, _VP, _DP, _VP]),
+    ("mm_normalize", _I, [_I, _SZ, _VP, _VP, _VP]),
+    ("mm_rk_prepare_step", _I, [_I, _SZ, _I, _D, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
+    ("mm_rk_combine_result", _I, [_I, _SZ, _I, _D, _DP, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
+    ("mm_round_tensor_dimension", _I, [_I, _I, _I]),
+    ("mm_demag_tensor", _I, [_I, _I, _I, _D, _D, _D, _I, _I, _I, _VP, _VP]),
+    ("mm_conv_create", _I, [ctypes.POINTER(_VP), _I, _I, _I, _I, _I, _I, _I, _VP, _VP]),
+    ("mm_conv_execute", _I, [_VP, _VP, _VP, _VP]),
+    ("mm_conv_destroy", _I, [_VP]),
+    ("mm_solver_create", _I, [ctypes.POINTER(_VP), ctypes.POINTER(mm_solver_config), _I,
+                              ctypes.POINTER(mm_material), _VP, _VP, _VP]),
+    ("mm_solver_destroy", _I, [_VP]),
+    ("mm_solver_set_M", _I, [_VP, _VP, _VP]),
+    ("mm_solver_get_M", _I, [_VP, _VP, _VP]),
+    ("mm_solver_set_time", _I, [_VP, _D, _D, _VP]),
+    ("mm_solver_step", _I, [_VP, _D, _VP]),
+    ("mm_solver_run", _I, [_VP, _D, _D, _DP, _DP, _I, ctypes.POINTER(_I), _VP]),
+    ("mm_solver_attempt", _I, [_VP, _D, _VP]),
+    ("mm_solver_eval", _I, [_VP, _VP, _VP, _VP, _VP]),
+    ("mm_solver_stats_get", _I, [_VP, ctypes.POINTER(mm_solver_stats), _VP]),
+    ("mm_solver_average_M", _I, [_VP, _DP, _VP]),
+]
+
+EXPORTED = [p[0] for p in _PROTOS]
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile libmmb200.so for sm_100a with nvcc (micromagnum_b200/csrc/Makefile)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", os.path.join(_HERE, "csrc"), "-j4"], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """The loaded library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with micromagnum_b200.build() "
+                "(nvcc, sm_100a); there is no CPU implementation")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _PROTOS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != MM_OK:
+        msg = lib().mm_last_error()
+        raise MMError(status, msg.decode() if msg else "")
+
+
+def launches() -> int:
+    return int(lib().mm_kernel_launch_count())

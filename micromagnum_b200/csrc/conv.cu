@@ -1,0 +1,618 @@
+// Demag convolution H = N * M, zero-padded to (px, py, pz), as shared-memory FFT passes over
+// HBM-resident spectra.  Replaces the reference's MatrixVectorConvolution_FFT::execute
+// (math/conv/MatrixVectorConvolution_FFT.cpp:110-375): pad, 3x R2C along x, transpose,
+// 3x C2C along y, transpose, 3x C2C along z, tensor multiply, and the inverses.
+//
+// B200 design:
+//  * no transposes: the y and z passes read tiles of TB consecutive x-frequencies per row, so
+//    every global access is a contiguous run of TB complex numbers;
+//  * zero padding is never stored: the x pass reads only the nx real samples of each row and
+//    writes only the rows y < ny, z < nz; the y pass pads in shared memory; the z pass pads,
+//    transforms, multiplies, inverse-transforms and writes back only z < nz;
+//  * two real rows share one complex FFT in the x passes (z = a + i b);
+//  * the tensor spectrum is real (Nxx, Nyy, Nzz even in every axis; Nxy, Nxz, Nyz odd in
+//    exactly two), so only Re N^ on ky <= py/2, kz <= pz/2 is stored, with the parity signs
+//    restored on the fly: 4x fewer tensor bytes than the reference's 12 complex matrices
+//    (SymmetricMatrixVectorConvolution_FFT.cpp:60-64 notes but does not use this);
+//  * for 2-D problems (nz == 1) the forward y FFT, the multiply and the inverse y FFT are one
+//    kernel.
+// Spectra layout: cplx<T> S[c][z][y][kx], c < 3, z < nz, y < py, kx < hx.
+#include "conv.cuh"
+
+#include <cmath>
+#include <vector>
+#include <algorithm>
+
+namespace mm {
+
+FftRadices fft_factor(int n)
+{
+	FftRadices f{};
+	f.n = n;
+	int m = n;
+	auto push = [&](int r) { f.r[f.count++] = r; m /= r; };
+	while (m % 8 == 0 && f.count < FFT_MAX_PASSES) push(8);
+	while (m % 4 == 0 && f.count < FFT_MAX_PASSES) push(4);
+	while (m % 2 == 0 && f.count < FFT_MAX_PASSES) push(2);
+	for (int p : {3, 5, 7})
+		while (m % p == 0 && f.count < FFT_MAX_PASSES) push(p);
+	for (int p = 11; m > 1 && f.count < FFT_MAX_PASSES; p += 2)
+		while (m % p == 0 && f.count < FFT_MAX_PASSES) push(p);
+	if (m != 1) f.count = -1;  // too many factors (cannot happen for n < 2^24)
+	return f;
+}
+
+namespace {
+
+constexpr int NT = 256;                 // threads per CTA for all passes
+constexpr size_t SMEM_TARGET = 100 * 1024;
+
+template <typename T>
+mm_status make_twiddles(int n, void **out)
+{
+	std::vector<cplx<T>> h(n);
+	for (int k = 0; k < n; ++k) {
+		const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)k / (long double)n;
+		h[k].x = (T)cosl(a);
+		h[k].y = (T)sinl(a);
+	}
+	MM_CUDA(cudaMalloc(out, sizeof(cplx<T>) * n));
+	MM_CUDA(cudaMemcpy(*out, h.data(), sizeof(cplx<T>) * n, cudaMemcpyHostToDevice));
+	return MM_OK;
+}
+
+template <typename T>
+__device__ __forceinline__ void load_twiddles(cplx<T> *tw_s, const cplx<T> *tw_g, int n)
+{
+	const int tid = threadIdx.x, nthr = blockDim.x;
+	for (int k = tid; k < n; k += nthr) tw_s[k] = tw_g[k];
+}
+
+// ---- x forward: real rows -> half spectra ------------------------------------------------------
+// Real row r = (c*nz + z)*ny + y is M[r*nx .. r*nx+nx); its spectrum goes to S row
+// (c*nz + z)*py + y.  Rows 2q and 2q+1 share complex line q.
+template <typename T, bool SCALE>
+__global__ void __launch_bounds__(NT) k_x_fwd(const T *__restrict__ M, const uint8_t *__restrict__ reg,
+                                             const T *__restrict__ ms_tab, cplx<T> *__restrict__ S,
+                                             int nx, int ny, int nz, int py, int hx, FftRadices rad,
+                                             const cplx<T> *__restrict__ tw_g, int LP)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int px = rad.n;
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + px;
+	C *b1 = b0 + (size_t)LP * px;
+	load_twiddles<T>(tw, tw_g, px);
+	const int rows = 3 * ny * nz;
+	const int nyz = ny * nz;
+	const int line0 = blockIdx.x * LP;
+	for (int e = threadIdx.x; e < LP * px; e += blockDim.x) {
+		const int b = e / px, x = e % px;
+		const int ra = 2 * (line0 + b), rb = ra + 1;
+		T a = 0, bb = 0;
+		if (x < nx) {
+			if (ra < rows) {
+				a = M[(size_t)ra * nx + x];
+				if (SCALE) a *= ms_tab[reg ? reg[(size_t)(ra % nyz) * nx + x] : 0];
+			}
+			if (rb < rows) {
+				bb = M[(size_t)rb * nx + x];
+				if (SCALE) bb *= ms_tab[reg ? reg[(size_t)(rb % nyz) * nx + x] : 0];
+			}
+		}
+		b0[e] = C{a, bb};
+	}
+	__syncthreads();
+	C *res = fft_lines<T, false>(b0, b1, px, 1, LP, rad, tw);
+	for (int e = threadIdx.x; e < LP * hx; e += blockDim.x) {
+		const int b = e / hx, k = e % hx;
+		const int ra = 2 * (line0 + b), rb = ra + 1;
+		const C zk = res[b * px + k];
+		const C zn = res[b * px + (px - k) % px];
+		const T h = T(0.5);
+		if (ra < rows) {
+			const int c = ra / nyz, rem = ra % nyz;
+			const size_t srow = (size_t)(c * nz + rem / ny) * py + rem % ny;
+			S[srow * hx + k] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
+		}
+		if (rb < rows) {
+			const int c = rb / nyz, rem = rb % nyz;
+			const size_t srow = (size_t)(c * nz + rem / ny) * py + rem % ny;
+			S[srow * hx + k] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
+		}
+	}
+}
+
+// ---- x inverse: half spectra -> real rows ------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_x_inv(const cplx<T> *__restrict__ S, T *__restrict__ H,
+                                             int nx, int ny, int nz, int py, int hx, FftRadices rad,
+                                             const cplx<T> *__restrict__ tw_g, int LP)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int px = rad.n;
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + px;
+	C *b1 = b0 + (size_t)LP * px;
+	load_twiddles<T>(tw, tw_g, px);
+	const int rows = 3 * ny * nz;
+	const int nyz = ny * nz;
+	const int line0 = blockIdx.x * LP;
+	const bool even = (px % 2) == 0;
+	for (int e = threadIdx.x; e < LP * px; e += blockDim.x) {
+		const int b = e / px, k = e % px;
+		const int ra = 2 * (line0 + b), rb = ra + 1;
+		const bool mirror = k >= hx;
+		const int kk = mirror ? px - k : k;
+		// the imaginary parts at kx = 0 and at the Nyquist frequency of a real row are zero
+		const bool realonly = (kk == 0) || (even && kk == px / 2);
+		C A = {0, 0}, B = {0, 0};
+		if (ra < rows) {
+			const int c = ra / nyz, rem = ra % nyz;
+			A = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * hx + kk];
+		}
+		if (rb < rows) {
+			const int c = rb / nyz, rem = rb % nyz;
+			B = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * hx + kk];
+		}
+		if (realonly) { A.y = 0; B.y = 0; }
+		if (mirror) { A.y = -A.y; B.y = -B.y; }
+		b0[e] = C{A.x - B.y, A.y + B.x};
+	}
+	__syncthreads();
+	C *res = fft_lines<T, true>(b0, b1, px, 1, LP, rad, tw);
+	for (int e = threadIdx.x; e < LP * nx; e += blockDim.x) {
+		const int b = e / nx, x = e % nx;
+		const int ra = 2 * (line0 + b), rb = ra + 1;
+		const C z = res[b * px + x];
+		if (ra < rows) H[(size_t)ra * nx + x] = z.x;
+		if (rb < rows) H[(size_t)rb * nx + x] = z.y;
+	}
+}
+
+// ---- y pass (3-D): column tiles, forward pads ny -> py, inverse crops py -> ny -----------------
+template <typename T, bool INV>
+__global__ void __launch_bounds__(NT) k_y(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
+                                         int py, int hx, FftRadices rad,
+                                         const cplx<T> *__restrict__ tw_g, int TB)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + py;
+	C *b1 = b0 + (size_t)TB * py;
+	load_twiddles<T>(tw, tw_g, py);
+	const int kx0 = blockIdx.x * TB;
+	const int z = blockIdx.y, c = blockIdx.z;
+	C *base = S + (size_t)(c * nz + z) * py * hx;
+	for (int e = threadIdx.x; e < TB * py; e += blockDim.x) {
+		const int y = e / TB, b = e % TB;
+		b0[e] = (y < n_in && kx0 + b < hx) ? base[(size_t)y * hx + kx0 + b] : C{0, 0};
+	}
+	__syncthreads();
+	C *res = fft_lines<T, INV>(b0, b1, 1, TB, TB, rad, tw);
+	for (int e = threadIdx.x; e < TB * n_out; e += blockDim.x) {
+		const int y = e / TB, b = e % TB;
+		if (kx0 + b < hx) base[(size_t)y * hx + kx0 + b] = res[e];
+	}
+}
+
+// Real tensor spectrum with parity signs restored.  t points at component 0 of
+// (kz', ky', kx); cs = component stride.
+template <typename T, typename C>
+__device__ __forceinline__ void tensor_apply(const T *__restrict__ t, size_t cs, T sy, T sz, C &m0,
+                                             C &m1, C &m2)
+{
+	const T nxx = t[0], nxy = sy * t[cs], nxz = sz * t[2 * cs];
+	const T nyy = t[3 * cs], nyz = sy * sz * t[4 * cs], nzz = t[5 * cs];
+	const C a = m0, b = m1, c = m2;
+	m0 = C{nxx * a.x + nxy * b.x + nxz * c.x, nxx * a.y + nxy * b.y + nxz * c.y};
+	m1 = C{nxy * a.x + nyy * b.x + nyz * c.x, nxy * a.y + nyy * b.y + nyz * c.y};
+	m2 = C{nxz * a.x + nyz * b.x + nzz * c.x, nxz * a.y + nyz * b.y + nzz * c.y};
+}
+
+// ---- z pass (3-D): forward FFT along z, tensor multiply, inverse FFT, all three components ----
+template <typename T>
+__global__ void __launch_bounds__(NT) k_z_mul(cplx<T> *__restrict__ S, const T *__restrict__ Nt,
+                                             int nz, int py, int hx, int qy, int qz, FftRadices rad,
+                                             const cplx<T> *__restrict__ tw_g, int TB)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int pz = rad.n;
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + pz;
+	C *b1 = b0 + (size_t)3 * TB * pz;
+	load_twiddles<T>(tw, tw_g, pz);
+	const int kx0 = blockIdx.x * TB;
+	const int ky = blockIdx.y;
+	const int L = 3 * TB;
+	const size_t cstride = (size_t)nz * py * hx;
+	for (int e = threadIdx.x; e < L * pz; e += blockDim.x) {
+		const int zz = e / L, l = e % L, c = l / TB, b = l % TB;
+		b0[e] = (zz < nz && kx0 + b < hx) ? S[c * cstride + ((size_t)zz * py + ky) * hx + kx0 + b] : C{0, 0};
+	}
+	__syncthreads();
+	C *res = fft_lines<T, false>(b0, b1, 1, L, L, rad, tw);
+	C *other = (res == b0) ? b1 : b0;
+	const bool fy = ky > py / 2;
+	const int kyr = fy ? py - ky : ky;
+	const T sy = fy ? T(-1) : T(1);
+	const size_t cs = (size_t)qz * qy * hx;
+	for (int e = threadIdx.x; e < pz * TB; e += blockDim.x) {
+		const int kz = e / TB, b = e % TB;
+		if (kx0 + b >= hx) continue;
+		const bool fz = kz > pz / 2;
+		const int kzr = fz ? pz - kz : kz;
+		const T sz = fz ? T(-1) : T(1);
+		const T *t = Nt + ((size_t)kzr * qy + kyr) * hx + kx0 + b;
+		C &m0 = res[kz * L + b], &m1 = res[kz * L + TB + b], &m2 = res[kz * L + 2 * TB + b];
+		tensor_apply<T, C>(t, cs, sy, sz, m0, m1, m2);
+	}
+	__syncthreads();
+	C *out = fft_lines<T, true>(res, other, 1, L, L, rad, tw);
+	for (int e = threadIdx.x; e < L * nz; e += blockDim.x) {
+		const int zz = e / L, l = e % L, c = l / TB, b = l % TB;
+		if (kx0 + b < hx) S[c * cstride + ((size_t)zz * py + ky) * hx + kx0 + b] = out[e];
+	}
+}
+
+// ---- y pass with multiply (2-D problems): forward y FFT, tensor multiply, inverse y FFT -------
+template <typename T>
+__global__ void __launch_bounds__(NT) k_y_mul2d(cplx<T> *__restrict__ S, const T *__restrict__ Nt,
+                                               int ny, int hx, int qy, FftRadices rad,
+                                               const cplx<T> *__restrict__ tw_g, int TB)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int py = rad.n;
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + py;
+	C *b1 = b0 + (size_t)3 * TB * py;
+	load_twiddles<T>(tw, tw_g, py);
+	const int kx0 = blockIdx.x * TB;
+	const int L = 3 * TB;
+	const size_t cstride = (size_t)py * hx;
+	for (int e = threadIdx.x; e < L * py; e += blockDim.x) {
+		const int y = e / L, l = e % L, c = l / TB, b = l % TB;
+		b0[e] = (y < ny && kx0 + b < hx) ? S[c * cstride + (size_t)y * hx + kx0 + b] : C{0, 0};
+	}
+	__syncthreads();
+	C *res = fft_lines<T, false>(b0, b1, 1, L, L, rad, tw);
+	C *other = (res == b0) ? b1 : b0;
+	const size_t cs = (size_t)qy * hx;  // qz == 1
+	for (int e = threadIdx.x; e < py * TB; e += blockDim.x) {
+		const int ky = e / TB, b = e % TB;
+		if (kx0 + b >= hx) continue;
+		const bool fy = ky > py / 2;
+		const int kyr = fy ? py - ky : ky;
+		const T sy = fy ? T(-1) : T(1);
+		const T *t = Nt + (size_t)kyr * hx + kx0 + b;
+		C &m0 = res[ky * L + b], &m1 = res[ky * L + TB + b], &m2 = res[ky * L + 2 * TB + b];
+		tensor_apply<T, C>(t, cs, sy, T(1), m0, m1, m2);
+	}
+	__syncthreads();
+	C *out = fft_lines<T, true>(res, other, 1, L, L, rad, tw);
+	for (int e = threadIdx.x; e < L * ny; e += blockDim.x) {
+		const int y = e / L, l = e % L, c = l / TB, b = l % TB;
+		if (kx0 + b < hx) S[c * cstride + (size_t)y * hx + kx0 + b] = out[e];
+	}
+}
+
+// ---- set-up: generic strided complex FFT (FP64) for the tensor spectrum ------------------------
+// The array is viewed as [outer][len][inner]; line (o, i) is data[o*len*inner + k*inner + i].
+template <typename T, bool INV>
+__global__ void __launch_bounds__(NT) k_fft_axis(cplx<T> *__restrict__ data, int inner, int outer,
+                                                FftRadices rad, const cplx<T> *__restrict__ tw_g,
+                                                int TB)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int len = rad.n;
+	C *tw = reinterpret_cast<C *>(smem_raw);
+	C *b0 = tw + len;
+	C *b1 = b0 + (size_t)TB * len;
+	load_twiddles<T>(tw, tw_g, len);
+	if (inner == 1) {
+		const int r0 = blockIdx.x * TB;
+		for (int e = threadIdx.x; e < TB * len; e += blockDim.x) {
+			const int b = e / len, k = e % len;
+			b0[e] = (r0 + b < outer) ? data[(size_t)(r0 + b) * len + k] : C{0, 0};
+		}
+		__syncthreads();
+		C *res = fft_lines<T, INV>(b0, b1, len, 1, TB, rad, tw);
+		for (int e = threadIdx.x; e < TB * len; e += blockDim.x) {
+			const int b = e / len, k = e % len;
+			if (r0 + b < outer) data[(size_t)(r0 + b) * len + k] = res[e];
+		}
+	} else {
+		const int i0 = blockIdx.x * TB;
+		const size_t o = blockIdx.y;
+		C *base = data + o * len * (size_t)inner;
+		for (int e = threadIdx.x; e < TB * len; e += blockDim.x) {
+			const int k = e / TB, b = e % TB;
+			b0[e] = (i0 + b < inner) ? base[(size_t)k * inner + i0 + b] : C{0, 0};
+		}
+		__syncthreads();
+		C *res = fft_lines<T, INV>(b0, b1, 1, TB, TB, rad, tw);
+		for (int e = threadIdx.x; e < TB * len; e += blockDim.x) {
+			const int k = e / TB, b = e % TB;
+			if (i0 + b < inner) base[(size_t)k * inner + i0 + b] = res[e];
+		}
+	}
+}
+
+__global__ void k_tensor_component(const double *__restrict__ N, double2 *__restrict__ X, size_t cnt, int comp)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+		X[i] = double2{N[i * 6 + comp], 0.0};
+}
+
+// Keeps Re of the spectrum on kx < hx, ky <= py/2, kz <= pz/2, scaled by 1/(px py pz), and
+// records max |Re| and max |Im| over the kept region (bit patterns of non-negative doubles).
+template <typename T>
+__global__ void k_tensor_extract(const double2 *__restrict__ X, T *__restrict__ out, int px, int py,
+                                 int hx, int qy, int qz, double scale, double *maxre, double *maxim)
+{
+	const size_t cnt = (size_t)qz * qy * hx;
+	double mr = 0, mi = 0;
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+		const int kx = (int)(i % hx);
+		const int ky = (int)((i / hx) % qy);
+		const int kz = (int)(i / ((size_t)hx * qy));
+		const double2 v = X[((size_t)kz * py + ky) * px + kx];
+		out[i] = (T)(v.x * scale);
+		mr = fmax(mr, fabs(v.x));
+		mi = fmax(mi, fabs(v.y));
+	}
+	block_max_to(maxre, mr);
+	block_max_to(maxim, mi);
+}
+
+int pick_tile(int len, int ncomp, size_t elem, int cap)
+{
+	int tb = cap;
+	while (tb > 1 && (size_t)(2 * ncomp * tb + 1) * len * elem > SMEM_TARGET) tb >>= 1;
+	return tb;
+}
+
+template <typename T>
+mm_status set_smem(const void *fn, size_t bytes)
+{
+	if (bytes > 48 * 1024)
+		MM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+	return MM_OK;
+}
+
+template <typename T>
+mm_status tensor_spectrum(ConvPlan *p, const double *N, cudaStream_t st)
+{
+	const int px = p->px, py = p->py, pz = p->pz;
+	const size_t cnt = (size_t)px * py * pz;
+	double2 *X = nullptr;
+	MM_CUDA(cudaMalloc(&X, cnt * sizeof(double2)));
+	void *twx = nullptr, *twy = nullptr, *twz = nullptr;
+	mm_status st_ = make_twiddles<double>(px, &twx);
+	if (st_ == MM_OK) st_ = make_twiddles<double>(py, &twy);
+	if (st_ == MM_OK) st_ = make_twiddles<double>(pz, &twz);
+	double *mx = nullptr;
+	if (st_ == MM_OK) st_ = cuda_status(cudaMalloc(&mx, 2 * sizeof(double)), "cudaMalloc");
+	if (st_ == MM_OK) st_ = cuda_status(cudaMemsetAsync(mx, 0, 2 * sizeof(double), st), "cudaMemsetAsync");
+	const double scale = 1.0 / ((double)px * py * pz);
+	const size_t per = (size_t)p->qz * p->qy * p->hx;
+	const int gsz = num_sms() * 8;
+	for (int comp = 0; comp < 6 && st_ == MM_OK; ++comp) {
+		k_tensor_component<<<gsz, NT, 0, st>>>(N, X, cnt, comp);
+		st_ = after_launch("k_tensor_component");
+		const int dims[3] = {px, py, pz};
+		const FftRadices rads[3] = {p->rx, p->ry, p->rz};
+		void *tws[3] = {twx, twy, twz};
+		size_t inner = 1, outer = (size_t)py * pz;
+		for (int ax = 0; ax < 3 && st_ == MM_OK; ++ax) {
+			const int len = dims[ax];
+			if (len > 1) {
+				const int TB = pick_tile(len, 1, sizeof(double2), inner == 1 ? 4 : 16);
+				const size_t smem = (size_t)(2 * TB + 1) * len * sizeof(double2);
+				st_ = set_smem<double>((const void *)k_fft_axis<double, false>, smem);
+				if (st_ != MM_OK) break;
+				dim3 grid;
+				if (inner == 1) grid = dim3((unsigned)((outer + TB - 1) / TB), 1, 1);
+				else grid = dim3((unsigned)((inner + TB - 1) / TB), (unsigned)outer, 1);
+				k_fft_axis<double, false><<<grid, NT, smem, st>>>(X, (int)inner, (int)outer, rads[ax],
+				                                                 (const double2 *)tws[ax], TB);
+				st_ = after_launch("k_fft_axis");
+			}
+			inner *= len;
+			outer = ax == 0 ? pz : 1;
+		}
+		if (st_ != MM_OK) break;
+		k_tensor_extract<T><<<gsz, NT, 0, st>>>(X, (T *)p->tensor + comp * per, px, py, p->hx, p->qy,
+		                                       p->qz, scale, mx, mx + 1);
+		st_ = after_launch("k_tensor_extract");
+	}
+	double hm[2] = {0, 0};
+	if (st_ == MM_OK) st_ = cuda_status(cudaMemcpyAsync(hm, mx, sizeof(hm), cudaMemcpyDeviceToHost, st), "cudaMemcpyAsync");
+	if (st_ == MM_OK) st_ = cuda_status(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+	p->max_imag_rel = hm[0] > 0 ? hm[1] / hm[0] : 0.0;
+	cudaFree(X);
+	cudaFree(twx);
+	cudaFree(twy);
+	cudaFree(twz);
+	cudaFree(mx);
+	return st_;
+}
+
+template <typename T>
+mm_status plan_setup(ConvPlan *p, const double *N, cudaStream_t st)
+{
+	using C = cplx<T>;
+	MM_TRY(make_twiddles<T>(p->px, &p->tw_x));
+	MM_TRY(make_twiddles<T>(p->py, &p->tw_y));
+	MM_TRY(make_twiddles<T>(p->pz, &p->tw_z));
+	MM_CUDA(cudaMalloc(&p->tensor, sizeof(T) * 6 * (size_t)p->qz * p->qy * p->hx));
+	MM_CUDA(cudaMalloc(&p->spec, p->spec_bytes()));
+	MM_CUDA(cudaMemsetAsync(p->spec, 0, p->spec_bytes(), st));
+	// launch geometry
+	{
+		int lp = 8;
+		while (lp > 1 && (size_t)(2 * lp + 1) * p->px * sizeof(C) > SMEM_TARGET) lp >>= 1;
+		p->lp_x = lp;
+		p->smem_x = (size_t)(2 * lp + 1) * p->px * sizeof(C);
+	}
+	if (p->is2d) {
+		p->tb_y = pick_tile(p->py, 3, sizeof(C), 32);
+		p->smem_y = (size_t)(6 * p->tb_y + 1) * p->py * sizeof(C);
+	} else {
+		p->tb_y = pick_tile(p->py, 1, sizeof(C), 32);
+		p->smem_y = (size_t)(2 * p->tb_y + 1) * p->py * sizeof(C);
+		p->tb_z = pick_tile(p->pz, 3, sizeof(C), 32);
+		p->smem_z = (size_t)(6 * p->tb_z + 1) * p->pz * sizeof(C);
+	}
+	if (p->smem_x > 227 * 1024 || p->smem_y > 227 * 1024 || p->smem_z > 227 * 1024)
+		return fail(MM_ERR_UNSUPPORTED, "conv: FFT length too large for one CTA");
+	MM_TRY(set_smem<T>((const void *)k_x_fwd<T, false>, p->smem_x));
+	MM_TRY(set_smem<T>((const void *)k_x_fwd<T, true>, p->smem_x));
+	MM_TRY(set_smem<T>((const void *)k_x_inv<T>, p->smem_x));
+	if (p->is2d) {
+		MM_TRY(set_smem<T>((const void *)k_y_mul2d<T>, p->smem_y));
+	} else {
+		MM_TRY(set_smem<T>((const void *)k_y<T, false>, p->smem_y));
+		MM_TRY(set_smem<T>((const void *)k_y<T, true>, p->smem_y));
+		MM_TRY(set_smem<T>((const void *)k_z_mul<T>, p->smem_z));
+	}
+	return tensor_spectrum<T>(p, N, st);
+}
+
+template <typename T>
+mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, T *H, cudaStream_t st)
+{
+	using C = cplx<T>;
+	C *S = (C *)p->spec;
+	const int rows = 3 * p->ny * p->nz;
+	const int lines = (rows + 1) / 2;
+	const int gx = (lines + p->lp_x - 1) / p->lp_x;
+	if (ms_tab)
+		k_x_fwd<T, true><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
+		                                            p->rx, (const C *)p->tw_x, p->lp_x);
+	else
+		k_x_fwd<T, false><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
+		                                             p->rx, (const C *)p->tw_x, p->lp_x);
+	MM_TRY(after_launch("k_x_fwd"));
+	if (p->is2d) {
+		const int gy = (p->hx + p->tb_y - 1) / p->tb_y;
+		k_y_mul2d<T><<<gy, NT, p->smem_y, st>>>(S, (const T *)p->tensor, p->ny, p->hx, p->qy, p->ry,
+		                                        (const C *)p->tw_y, p->tb_y);
+		MM_TRY(after_launch("k_y_mul2d"));
+	} else {
+		dim3 gy((p->hx + p->tb_y - 1) / p->tb_y, p->nz, 3);
+		k_y<T, false><<<gy, NT, p->smem_y, st>>>(S, p->ny, p->py, p->nz, p->py, p->hx, p->ry,
+		                                         (const C *)p->tw_y, p->tb_y);
+		MM_TRY(after_launch("k_y_fwd"));
+		dim3 gz((p->hx + p->tb_z - 1) / p->tb_z, p->py, 1);
+		k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz,
+		                                      p->rz, (const C *)p->tw_z, p->tb_z);
+		MM_TRY(after_launch("k_z_mul"));
+		k_y<T, true><<<gy, NT, p->smem_y, st>>>(S, p->py, p->ny, p->nz, p->py, p->hx, p->ry,
+		                                        (const C *)p->tw_y, p->tb_y);
+		MM_TRY(after_launch("k_y_inv"));
+	}
+	k_x_inv<T><<<gx, NT, p->smem_x, st>>>(S, H, p->nx, p->ny, p->nz, p->py, p->hx, p->rx,
+	                                      (const C *)p->tw_x, p->lp_x);
+	return after_launch("k_x_inv");
+}
+
+} // namespace
+
+size_t ConvPlan::spec_bytes() const
+{
+	const size_t c = prec == MM_F64 ? sizeof(double2) : sizeof(float2);
+	return c * 3 * (size_t)nz * py * hx;
+}
+
+ConvPlan::~ConvPlan()
+{
+	cudaFree(tw_x);
+	cudaFree(tw_y);
+	cudaFree(tw_z);
+	cudaFree(tensor);
+	cudaFree(spec);
+}
+
+int conv_launches(const ConvPlan *p) { return p->is2d ? 3 : 5; }
+
+mm_status conv_plan_create(ConvPlan **out, int prec, int nx, int ny, int nz, int px, int py, int pz,
+                           const double *N, cudaStream_t st)
+{
+	if (prec != MM_F64 && prec != MM_F32) return fail(MM_ERR_INVALID_ARGUMENT, "conv: bad precision");
+	if (nx <= 0 || ny <= 0 || nz <= 0 || px < nx || py < ny || pz < nz || !N)
+		return fail(MM_ERR_INVALID_ARGUMENT, "conv: invalid sizes or null tensor");
+	ConvPlan *p = new ConvPlan();
+	p->prec = prec;
+	p->nx = nx; p->ny = ny; p->nz = nz;
+	p->px = px; p->py = py; p->pz = pz;
+	p->hx = px / 2 + 1;
+	p->qy = py / 2 + 1;
+	p->qz = pz / 2 + 1;
+	p->is2d = (nz == 1 && pz == 1);
+	p->rx = fft_factor(px);
+	p->ry = fft_factor(py);
+	p->rz = fft_factor(pz);
+	if (p->rx.count < 0 || p->ry.count < 0 || p->rz.count < 0) {
+		delete p;
+		return fail(MM_ERR_UNSUPPORTED, "conv: FFT length has too many prime factors");
+	}
+	const mm_status s = prec == MM_F64 ? plan_setup<double>(p, N, st) : plan_setup<float>(p, N, st);
+	if (s != MM_OK) {
+		delete p;
+		return s;
+	}
+	*out = p;
+	return MM_OK;
+}
+
+mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const void *ms_table,
+                       void *H, cudaStream_t st)
+{
+	if (p->prec == MM_F64)
+		return execute<double>(p, (const double *)M, regions, (const double *)ms_table, (double *)H, st);
+	return execute<float>(p, (const float *)M, regions, (const float *)ms_table, (float *)H, st);
+}
+
+} // namespace mm
+
+struct mm_conv {
+	mm::ConvPlan *plan;
+};
+
+using namespace mm;
+
+extern "C" {
+
+MM_API mm_status mm_conv_create(mm_conv **out, int prec, int nx, int ny, int nz, int ex, int ey,
+                                int ez, const double *N_device, void *stream)
+{
+	if (!out) return fail(MM_ERR_INVALID_ARGUMENT, "mm_conv_create: null out");
+	ConvPlan *p = nullptr;
+	MM_TRY(conv_plan_create(&p, prec, nx, ny, nz, ex, ey, ez, N_device, as_stream(stream)));
+	*out = new mm_conv{p};
+	return MM_OK;
+}
+
+MM_API mm_status mm_conv_execute(mm_conv *conv, const void *M, void *H, void *stream)
+{
+	if (!conv || !conv->plan || !M || !H) return fail(MM_ERR_INVALID_ARGUMENT, "mm_conv_execute: null argument");
+	return conv_execute(conv->plan, M, nullptr, nullptr, H, as_stream(stream));
+}
+
+MM_API mm_status mm_conv_destroy(mm_conv *conv)
+{
+	if (conv) {
+		delete conv->plan;
+		delete conv;
+	}
+	return MM_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,45 @@
+// Zero-padded FFT convolution H = N * M with the symmetric demag tensor (internal API).
+#pragma once
+
+#include "mm_common.cuh"
+#include "fft.cuh"
+
+namespace mm {
+
+struct ConvPlan {
+	int prec = MM_F64;
+	int nx = 0, ny = 0, nz = 0;     // grid
+	int px = 0, py = 0, pz = 0;     // padded (FFT) lengths
+	int hx = 0;                     // px/2 + 1 stored x frequencies
+	int qy = 0, qz = 0;             // py/2 + 1, pz/2 + 1 stored tensor frequencies
+	bool is2d = false;              // nz == 1 && pz == 1
+	FftRadices rx{}, ry{}, rz{};
+	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
+	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]
+	void *spec = nullptr;           // cplx<T>[3][nz][py][hx]
+	// launch geometry
+	int lp_x = 1;                   // complex lines (= 2 real rows) per CTA in the x passes
+	int tb_y = 1, tb_z = 1;         // columns per CTA in the y and z passes
+	size_t smem_x = 0, smem_y = 0, smem_z = 0;
+	double max_imag_rel = 0.0;      // largest |Im N^| / max |Re N^| seen at set-up
+
+	size_t spec_bytes() const;
+	~ConvPlan();
+};
+
+// Builds the plan and the tensor spectrum from an FP64 tensor in the reference layout
+// (component fastest, then x, y, z) of padded size px*py*pz.
+mm_status conv_plan_create(ConvPlan **out, int prec, int nx, int ny, int nz, int px, int py,
+                           int pz, const double *N_device, cudaStream_t st);
+
+// H = N * (Ms[region] * M) when regions/ms_table are given, else H = N * M.
+// M and H are SoA arrays of T (T = double for MM_F64, float for MM_F32).
+mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const void *ms_table,
+                       void *H, cudaStream_t st);
+
+// Number of kernel launches one conv_execute issues.
+int conv_launches(const ConvPlan *p);
+
+FftRadices fft_factor(int n);
+
+} // namespace mm

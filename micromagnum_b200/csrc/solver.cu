@@ -1,0 +1,1046 @@
+// The fused B200 solver: Runge-Kutta steps of the Landau-Lifshitz-Gilbert equation with the
+// reference's step controller, entirely on the device.
+//
+// Reference path replaced (per RK stage): magnum/evolver/runge_kutta.py:105-118 forms the stage
+// state with one axpy per earlier stage, then LandauLifshitzGilbert.calculate_dMdt
+// (landau_lifshitz_gilbert.py:92-125) fills H_tot with one kernel per field term (stray field
+// convolution, exchange, anisotropy, applied field), adds them with axpys, calls llge and adds
+// the Zhang-Li torque; the step ends with rk_combine_result / Python axpys, two scaled_abs_max
+// reductions with host synchronisation (micro_magnetics_stepsize_controller.py:35-73) and a
+// normalisation (micro_magnetics.py:49-50).
+//
+// Here each stage is: the demag convolution passes (conv.cu) + ONE fused kernel that evaluates
+// exchange, anisotropy, applied field, LLG and Zhang-Li for a cell, writes k_i and the next stage
+// state, and (first/last stages) folds the |k_0| and error maxima into device reductions.  A
+// one-thread controller kernel applies the reference's accept/reject rule on the device.
+//
+// State representation: unit magnetisation m = M/Ms (Ms per region), which is the reference's
+// ODE scaled cell-wise by the constant 1/Ms: the Runge-Kutta combinations are linear, so the
+// trajectory and the controller's scaled errors (|y_err|/Ms) are the same quantities.  Material
+// parameters are a per-region table (<= 256 regions, one uint8 index per cell).
+//
+// Precision modes: MM_F64 is plain double.  MM_F32 computes fields, stages and reductions in
+// float and keeps the state as an unevaluated float pair m = hi + lo that is updated with an
+// error-free two-sum (a compensated update), so the accumulated state is not limited by float
+// rounding of the per-step increment; the controller runs in double.
+#include "mm_common.cuh"
+#include "conv.cuh"
+
+#include <vector>
+#include <cstring>
+#include <cmath>
+
+namespace mm {
+
+template <typename T>
+struct DevMat {
+	T Ms;        // saturation magnetisation
+	T cex;       // 2 A / (mu0 Ms)                       exchange prefactor
+	T l1, l2;    // LLG on unit m: dm = l1 m x H + l2 m x (m x H)
+	T ku;        // 2 k_u / (mu0 Ms)                     uniaxial
+	T kc;        // -2 k_c / (mu0 Ms)                    cubic
+	T zl1, zl2;  // Zhang-Li on unit m: dm = zl1 m x (m x u') + zl2 m x u', u' = (j.grad)M / Ms
+	T a1[3], a2[3], a3[3];
+	T j[3];
+};
+
+struct DevState {
+	double t;         // time at the start of the attempt
+	double h;         // step size of the attempt
+	double max_err2;  // max |m_err|^2 of the attempt (reduction)
+	double max_k02;   // max |k_0|^2 of the attempt (reduction)
+	double h_new;     // controller output
+	int accept;
+	int not_finite;
+	int pad[2];
+};
+
+constexpr int MAXS = 8;
+
+template <typename T>
+struct KTab {
+	T *k[MAXS];
+};
+
+struct Tableau {
+	int s, order, fsal;
+	double a[MAXS], b[MAXS][MAXS], c[MAXS], ec[MAXS];
+};
+
+// magnum/evolver/tableaus.py:54-139
+static Tableau make_tableau(int which)
+{
+	Tableau t{};
+	if (which == MM_RK_DP54) {
+		t.s = 7; t.order = 5; t.fsal = 1;
+		const double a[7] = {0.0, 1.0 / 5.0, 3.0 / 10.0, 4.0 / 5.0, 8.0 / 9.0, 1.0, 1.0};
+		const double b[7][6] = {{0},
+		                        {1.0 / 5.0},
+		                        {3.0 / 40.0, 9.0 / 40.0},
+		                        {44.0 / 45.0, -56.0 / 15.0, 32.0 / 9.0},
+		                        {19372.0 / 6561.0, -25360.0 / 2187.0, 64448.0 / 6561.0, -212.0 / 729.0},
+		                        {9017.0 / 3168.0, -355.0 / 33.0, 46732.0 / 5247.0, 49.0 / 176.0, -5103.0 / 18656.0},
+		                        {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0}};
+		const double c4[7] = {5179.0 / 57600.0, 0.0, 7571.0 / 16695.0, 393.0 / 640.0, -92097.0 / 339200.0, 187.0 / 2100.0, 1.0 / 40.0};
+		const double c5[7] = {35.0 / 384.0, 0.0, 500.0 / 1113.0, 125.0 / 192.0, -2187.0 / 6784.0, 11.0 / 84.0, 0.0};
+		for (int i = 0; i < 7; ++i) {
+			t.a[i] = a[i];
+			for (int j = 0; j < 6; ++j) t.b[i][j] = b[i][j];
+			t.c[i] = c5[i];
+			t.ec[i] = c4[i] - c5[i];
+		}
+	} else if (which == MM_RK_RKF45) {
+		t.s = 6; t.order = 4; t.fsal = 0;
+		const double a[6] = {0.0, 1.0 / 4.0, 3.0 / 8.0, 12.0 / 13.0, 1.0, 1.0 / 2.0};
+		const double b[6][5] = {{0},
+		                        {1.0 / 4.0},
+		                        {3.0 / 32.0, 9.0 / 32.0},
+		                        {1932.0 / 2197.0, -7200.0 / 2197.0, 7296.0 / 2197.0},
+		                        {439.0 / 216.0, -8.0, 3680.0 / 513.0, -845.0 / 4104.0},
+		                        {-8.0 / 27.0, 2.0, -3544.0 / 2565.0, 1859.0 / 4104.0, -11.0 / 40.0}};
+		const double c4[6] = {25.0 / 216.0, 0.0, 1408.0 / 2565.0, 2197.0 / 4104.0, -1.0 / 5.0, 0.0};
+		const double c5[6] = {16.0 / 135.0, 0.0, 6656.0 / 12825.0, 28561.0 / 56430.0, -9.0 / 50.0, 2.0 / 55.0};
+		for (int i = 0; i < 6; ++i) {
+			t.a[i] = a[i];
+			for (int j = 0; j < 5; ++j) t.b[i][j] = b[i][j];
+			t.c[i] = c4[i];
+			t.ec[i] = c4[i] - c5[i];
+		}
+	} else if (which == MM_RK_CC45) {
+		t.s = 6; t.order = 4; t.fsal = 0;
+		const double a[6] = {0.0, 1.0 / 5.0, 3.0 / 10.0, 3.0 / 5.0, 1.0, 7.0 / 8.0};
+		const double b[6][5] = {{0},
+		                        {1.0 / 5.0},
+		                        {3.0 / 40.0, 9.0 / 40.0},
+		                        {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0},
+		                        {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0},
+		                        {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0}};
+		const double c4[6] = {2825.0 / 27648.0, 0.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
+		const double c5[6] = {37.0 / 378.0, 0.0, 250.0 / 621.0, 125.0 / 594.0, 0.0, 512.0 / 1771.0};
+		for (int i = 0; i < 6; ++i) {
+			t.a[i] = a[i];
+			for (int j = 0; j < 5; ++j) t.b[i][j] = b[i][j];
+			t.c[i] = c4[i];
+			t.ec[i] = c4[i] - c5[i];
+		}
+	} else {  // rk23
+		t.s = 4; t.order = 3; t.fsal = 1;
+		const double a[4] = {0.0, 0.5, 3.0 / 4.0, 1.0};
+		const double b[4][3] = {{0}, {1.0 / 2.0}, {0.0, 3.0 / 4.0}, {2.0 / 9.0, 1.0 / 3.0, 4.0 / 9.0}};
+		const double c2[4] = {7.0 / 24.0, 1.0 / 4.0, 1.0 / 3.0, 1.0 / 8.0};
+		const double c3[4] = {2.0 / 9.0, 1.0 / 3.0, 4.0 / 9.0, 0.0};
+		for (int i = 0; i < 4; ++i) {
+			t.a[i] = a[i];
+			for (int j = 0; j < 3; ++j) t.b[i][j] = b[i][j];
+			t.c[i] = c3[i];
+			t.ec[i] = c2[i] - c3[i];
+		}
+	}
+	return t;
+}
+
+// Arguments shared by the per-cell kernels.
+template <typename T>
+struct CellArgs {
+	int nx, ny, nz;
+	T wx, wy, wz;                  // 1/dx^2 ...
+	T idx2, idy2, idz2;            // 1/(2 dx) ... (Zhang-Li central differences)
+	T idx1, idy1, idz1;            // 1/dx ...     (one-sided differences)
+	int terms;
+	const uint8_t *reg;            // nullptr: every cell is region 0
+	const DevMat<T> *mat;
+	double Hext[3], Hpulse[3], rise;
+};
+
+template <typename T>
+__device__ __forceinline__ const DevMat<T> &mat_of(const CellArgs<T> &a, size_t i)
+{
+	return a.mat[a.reg ? a.reg[i] : 0];
+}
+
+// Effective field (without the demag term) and dm/dt of one cell of the unit-m field y.
+// Hd: demag field of the cell (added when the term is on).  Returns false for empty cells.
+template <typename T>
+__device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restrict__ y, size_t n,
+                                         int x, int yy, int z, size_t i, V3<T> Hd, double t,
+                                         V3<T> &Heff, V3<T> &dm)
+{
+	const DevMat<T> &M = mat_of(a, i);
+	if (M.Ms == T(0)) {
+		Heff = v3<T>(0, 0, 0);
+		dm = v3<T>(0, 0, 0);
+		return false;
+	}
+	const V3<T> m = load3(y, i, n);
+	const size_t nxy = (size_t)a.nx * a.ny;
+	V3<T> H = (a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0);
+	// neighbour indices (valid flags)
+	const bool hl = x > 0, hr = x < a.nx - 1, hd = yy > 0, hu = yy < a.ny - 1, hb = z > 0, hf = z < a.nz - 1;
+	if (a.terms & MM_TERM_EXCHANGE) {
+		// exchange_cpu.cpp:60-139: H = 2A/(mu0 Ms) sum_nb w (m_nb - m), empty neighbours skipped
+		V3<T> s = v3<T>(0, 0, 0);
+		auto nb = [&](bool ok, size_t j, T w) {
+			if (ok && mat_of(a, j).Ms != T(0)) s = s + w * (load3(y, j, n) - m);
+		};
+		nb(hl, i - 1, a.wx);
+		nb(hr, i + 1, a.wx);
+		nb(hd, i - a.nx, a.wy);
+		nb(hu, i + a.nx, a.wy);
+		nb(hb, i - nxy, a.wz);
+		nb(hf, i + nxy, a.wz);
+		H = H + M.cex * s;
+	}
+	if (a.terms & MM_TERM_UNIAXIAL) {
+		// anisotropy_cpu.cpp:29-73 (k == 0 gives ku == 0)
+		const V3<T> ax = v3<T>(M.a1[0], M.a1[1], M.a1[2]);
+		H = H + (M.ku * dot(m, ax)) * ax;
+	}
+	if (a.terms & MM_TERM_CUBIC) {
+		// anisotropy_cpu.cpp:75-119 on m/|m|
+		const T len = sqrt(dot(m, m));
+		const V3<T> u = len > T(0) ? (T(1) / len) * m : v3<T>(0, 0, 0);
+		const V3<T> u1 = v3<T>(M.a1[0], M.a1[1], M.a1[2]), u2 = v3<T>(M.a2[0], M.a2[1], M.a2[2]),
+		            u3 = v3<T>(M.a3[0], M.a3[1], M.a3[2]);
+		const T p1 = dot(u1, u), p2 = dot(u2, u), p3 = dot(u3, u);
+		const T s1 = p1 * p1, s2 = p2 * p2, s3 = p3 * p3;
+		H = H + M.kc * (((s2 + s3) * p1) * u1 + ((s1 + s3) * p2) * u2 + ((s1 + s2) * p3) * u3);
+	}
+	if (a.terms & MM_TERM_ZEEMAN) {
+		double f = 1.0;
+		if (a.rise > 0) f = t / a.rise < 1.0 ? t / a.rise : 1.0;
+		H = H + v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
+		              (T)(a.Hext[2] + a.Hpulse[2] * f));
+	}
+	Heff = H;
+	// llge_cpu.cpp:25-45 on unit m
+	const V3<T> mxh = cross(m, H);
+	dm = M.l1 * mxh + M.l2 * cross(m, mxh);
+	if (a.terms & MM_TERM_ZHANGLI) {
+		// fdm_zhangli_cpu.cpp:100-200: u = (j.grad)M from raw M = Ms m (no Ms masking),
+		// one-sided at the borders, zero along a dimension of size 1
+		auto Mv = [&](size_t j) { return mat_of(a, j).Ms * load3(y, j, n); };
+		const V3<T> Mc = M.Ms * m;
+		auto grad = [&](int c, int dim, size_t stride, T inv1, T inv2) -> V3<T> {
+			if (dim <= 1) return v3<T>(0, 0, 0);
+			if (c == 0) return inv1 * (Mv(i + stride) - Mc);
+			if (c == dim - 1) return inv1 * (Mc - Mv(i - stride));
+			return inv2 * (Mv(i + stride) - Mv(i - stride));
+		};
+		const V3<T> gx = grad(x, a.nx, 1, a.idx1, a.idx2);
+		const V3<T> gy = grad(yy, a.ny, a.nx, a.idy1, a.idy2);
+		const V3<T> gz = grad(z, a.nz, nxy, a.idz1, a.idz2);
+		const T inv = T(1) / M.Ms;
+		const V3<T> u = inv * v3<T>(M.j[0] * gx.x + M.j[1] * gy.x + M.j[2] * gz.x,
+		                            M.j[0] * gx.y + M.j[1] * gy.y + M.j[2] * gz.y,
+		                            M.j[0] * gx.z + M.j[1] * gy.z + M.j[2] * gz.z);
+		const V3<T> mxu = cross(m, u);
+		dm = dm + M.zl1 * cross(m, mxu) + M.zl2 * mxu;
+	}
+	return true;
+}
+
+// Per-stage coefficients (by value).
+struct StageCoef {
+	int stage;        // i
+	int last;         // i == s-1
+	int write_next;   // not last: write y_{i+1}
+	int write_new;    // last: write y_{n+1} (always in MM_F32, non-FSAL in MM_F64)
+	int reduce_k0;    // fold max |k_0|^2
+	double a_i;       // time node of this stage
+	double bn[MAXS];  // b[i+1][0..i] (not last)  or  c[0..s-1] (last)
+	double ec[MAXS];  // error weights (last)
+};
+
+// One fused stage: k_i = f(y_in) (demag field from Hd), then the next stage state
+// y_{i+1} = y_n + h sum_{l<=i} b_{i+1,l} k_l, or on the last stage the error maximum and y_{n+1}.
+// COMP: compensated float state (y_n = yhi + ylo).
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
+                                               const T *__restrict__ y_in, const T *__restrict__ Hd,
+                                               const T *__restrict__ yhi, const T *__restrict__ ylo,
+                                               const KTab<T> *__restrict__ ktab, T *__restrict__ y_out,
+                                               T *__restrict__ y_out_lo, const DevState *__restrict__ st,
+                                               double *red_err, double *red_k0)
+{
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	const bool inside = x < a.nx && yy < a.ny;
+	const size_t n = (size_t)a.nx * a.ny * a.nz;
+	const size_t i = ((size_t)z * a.ny + (inside ? yy : 0)) * a.nx + (inside ? x : 0);
+	const double h = st->h;
+	T e2 = T(0), k02 = T(0);
+	if (inside) {
+		V3<T> Heff, ki;
+		const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, i, n) : v3<T>(0, 0, 0);
+		cell_rhs<T>(a, y_in, n, x, yy, z, i, hd, st->t + sc.a_i * h, Heff, ki);
+		T *const *K = ktab->k;
+		store3(K[sc.stage], i, n, ki);
+		if (!sc.last) {
+			if (sc.write_next) {
+				V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
+				for (int l = 0; l < sc.stage; ++l) {
+					const T f = (T)(h * sc.bn[l]);
+					if (f != T(0)) acc = acc + f * load3(K[l], i, n);
+				}
+				acc = acc + (T)(h * sc.bn[sc.stage]) * ki;
+				if (COMP) acc = load3(yhi, i, n) + acc;
+				store3(y_out, i, n, acc);
+			}
+			if (sc.reduce_k0) {
+				const V3<T> k0 = sc.stage == 0 ? ki : load3(K[0], i, n);
+				k02 = dot(k0, k0);
+			}
+		} else {
+			V3<T> err = v3<T>(0, 0, 0);
+			V3<T> acc = v3<T>(0, 0, 0);
+			for (int l = 0; l <= sc.stage; ++l) {
+				const T fe = (T)(h * sc.ec[l]);
+				const T fc = (T)(h * sc.bn[l]);
+				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
+				const V3<T> kl = l == sc.stage ? ki : load3(K[l], i, n);
+				err = err + fe * kl;
+				if (sc.write_new) acc = acc + fc * kl;
+			}
+			e2 = dot(err, err);
+			if (sc.write_new) {
+				if (COMP) {
+					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
+					const V3<T> hi = load3(yhi, i, n);
+					const V3<T> d = load3(ylo, i, n) + acc;
+					const V3<T> s = hi + d;
+					const V3<T> bb = s - hi;
+					const V3<T> lo = (hi - (s - bb)) + (d - bb);
+					store3(y_out, i, n, s);
+					store3(y_out_lo, i, n, lo);
+				} else {
+					store3(y_out, i, n, load3(yhi, i, n) + acc);
+				}
+			}
+		}
+	}
+	if (sc.last) block_max_to(red_err, e2);
+	if (sc.reduce_k0) block_max_to(red_k0, k02);
+}
+
+// Accepted step: m <- y_{n+1} / |y_{n+1}| (VectorMatrix::normalize to Ms, in unit form).
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_accept(size_t n, const T *__restrict__ ynew,
+                                                const T *__restrict__ ynew_lo, T *__restrict__ m,
+                                                T *__restrict__ m_lo)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+		if (COMP) {
+			const double x = (double)ynew[i] + (double)ynew_lo[i];
+			const double y = (double)ynew[i + n] + (double)ynew_lo[i + n];
+			const double z = (double)ynew[i + 2 * n] + (double)ynew_lo[i + 2 * n];
+			const double len = sqrt(x * x + y * y + z * z);
+			const double s = len > 0 ? 1.0 / len : 0.0;
+			const double v[3] = {x * s, y * s, z * s};
+			for (int c = 0; c < 3; ++c) {
+				const float hi = (float)v[c];
+				m[i + c * n] = hi;
+				m_lo[i + c * n] = (float)(v[c] - (double)hi);
+			}
+		} else {
+			const V3<T> v = load3(ynew, i, n);
+			const T len = sqrt(dot(v, v));
+			store3(m, i, n, len > T(0) ? (T(1) / len) * v : v3<T>(0, 0, 0));
+		}
+	}
+}
+
+// MicroMagneticsStepSizeController.adjust_stepsize (micro_magnetics_stepsize_controller.py:
+// 35-73), in double, on one thread; also swaps k_0 / k_last for first-same-as-last tableaus.
+template <typename T>
+__global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double eps_rel, int order,
+                             int fsal, int s, DevState *host_copy)
+{
+	const double h = st->h;
+	const double e_abs = sqrt(st->max_err2);
+	const double max_dydt = sqrt(st->max_k02);
+	int accept;
+	double h_new;
+	const int finite = isfinite(e_abs) && isfinite(max_dydt);
+	if (h * max_dydt == 0.0) {
+		accept = 1;
+		h_new = 5e-14;
+	} else {
+		const double e_rel = e_abs / (h * max_dydt);
+		accept = (e_abs <= eps_abs) && (e_rel <= eps_rel);
+		// e_abs == 0 (ZeroDivisionError in the reference) grows the step by the maximum factor
+		const double sa = e_abs > 0 ? 0.85 * pow(eps_abs / e_abs, 1.0 / (order + 1.0)) : 5.0;
+		const double sr = e_rel > 0 ? 0.85 * pow(eps_rel / e_rel, 1.0 / order) : 5.0;
+		double sc = fmin(sa, sr);
+		sc = fmin(fmax(sc, 0.2), 5.0);
+		h_new = fmin(fmax(h * sc, 1e-15), 1e-10);
+		if (h_new == 1e-15) accept = 1;
+	}
+	if (!finite) accept = 0;
+	st->accept = accept;
+	st->h_new = h_new;
+	st->not_finite = !finite;
+	*host_copy = *st;
+	st->max_err2 = 0.0;
+	st->max_k02 = 0.0;
+	if (fsal) {
+		T *t = ktab->k[0];
+		ktab->k[0] = ktab->k[s - 1];
+		ktab->k[s - 1] = t;
+	}
+}
+
+// Effective field and dM/dt in A/m (FP64 outputs) at the state m.
+template <typename T>
+__global__ void __launch_bounds__(256) k_eval(CellArgs<T> a, const T *__restrict__ m,
+                                              const T *__restrict__ Hd, double t,
+                                              double *__restrict__ Heff_out,
+                                              double *__restrict__ dMdt_out,
+                                              double *__restrict__ Hd_out)
+{
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	if (x >= a.nx || yy >= a.ny) return;
+	const size_t n = (size_t)a.nx * a.ny * a.nz;
+	const size_t i = ((size_t)z * a.ny + yy) * a.nx + x;
+	V3<T> Heff, dm;
+	const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, i, n) : v3<T>(0, 0, 0);
+	cell_rhs<T>(a, m, n, x, yy, z, i, hd, t, Heff, dm);
+	const double ms = (double)mat_of(a, i).Ms;
+	if (Heff_out) { Heff_out[i] = Heff.x; Heff_out[i + n] = Heff.y; Heff_out[i + 2 * n] = Heff.z; }
+	if (dMdt_out) { dMdt_out[i] = ms * dm.x; dMdt_out[i + n] = ms * dm.y; dMdt_out[i + 2 * n] = ms * dm.z; }
+	if (Hd_out) { Hd_out[i] = hd.x; Hd_out[i + n] = hd.y; Hd_out[i + 2 * n] = hd.z; }
+}
+
+// M (A/m, FP64) -> unit state, normalised (LandauLifshitzGilbert.update("M")).
+template <typename T, bool COMP>
+__global__ void k_set_M(size_t n, const double *__restrict__ M, const uint8_t *__restrict__ reg,
+                        const DevMat<T> *__restrict__ mat, T *__restrict__ m, T *__restrict__ m_lo)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+		const double ms = (double)mat[reg ? reg[i] : 0].Ms;
+		const double x = M[i], y = M[i + n], z = M[i + 2 * n];
+		const double len = sqrt(x * x + y * y + z * z);
+		const double s = (ms != 0.0 && len > 0) ? 1.0 / len : 0.0;
+		const double v[3] = {x * s, y * s, z * s};
+		for (int c = 0; c < 3; ++c) {
+			const T hi = (T)v[c];
+			m[i + c * n] = hi;
+			if (COMP) m_lo[i + c * n] = (T)(v[c] - (double)hi);
+		}
+	}
+}
+
+template <typename T, bool COMP>
+__global__ void k_get_M(size_t n, const T *__restrict__ m, const T *__restrict__ m_lo,
+                        const uint8_t *__restrict__ reg, const DevMat<T> *__restrict__ mat,
+                        double *__restrict__ M)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+		const double ms = (double)mat[reg ? reg[i] : 0].Ms;
+		for (int c = 0; c < 3; ++c) {
+			double v = (double)m[i + c * n];
+			if (COMP) v += (double)m_lo[i + c * n];
+			M[i + c * n] = ms * v;
+		}
+	}
+}
+
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_average_M(size_t n, const T *__restrict__ m, const T *__restrict__ m_lo,
+                                                   const uint8_t *__restrict__ reg,
+                                                   const DevMat<T> *__restrict__ mat, double *out3)
+{
+	double s[3] = {0, 0, 0};
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+		const double ms = (double)mat[reg ? reg[i] : 0].Ms;
+		for (int c = 0; c < 3; ++c) {
+			double v = (double)m[i + c * n];
+			if (COMP) v += (double)m_lo[i + c * n];
+			s[c] += ms * v;
+		}
+	}
+	for (int c = 0; c < 3; ++c) block_sum_to(out3 + c, s[c]);
+}
+
+} // namespace mm
+
+using namespace mm;
+
+struct mm_solver {
+	mm_solver_config cfg{};
+	size_t n = 0;
+	int px = 0, py = 0, pz = 0;
+	Tableau tab{};
+	ConvPlan *conv = nullptr;
+	void *mat = nullptr;           // DevMat<T>[nmat]
+	void *ms_tab = nullptr;        // T[nmat] (Ms per region, for the demag input)
+	uint8_t *reg = nullptr;
+	void *m = nullptr, *m_lo = nullptr;        // state (unit), low part (F32)
+	void *ys[2] = {nullptr, nullptr};          // stage state ping-pong
+	void *ynew_lo = nullptr;                   // F32: low part of y_{n+1}
+	void *k[MAXS] = {};
+	void *hd = nullptr;                        // demag field
+	void *ktab = nullptr;                      // KTab<T> on device
+	DevState *dst = nullptr;                   // device state
+	DevState *hst = nullptr;                   // pinned host copy of the controller output
+	double *avg = nullptr;                     // device scratch for <M>
+	double *avg_h = nullptr;                   // pinned
+	int last_stage_buf = 0;                    // ys[] index holding y_{n+1}
+	// host-side solver state (RungeKutta.evolve semantics, runge_kutta.py:47-87)
+	double t = 0, h = 0, h_next = 0;
+	bool have_next = false;
+	bool k0_valid = false;
+	int64_t steps = 0, attempts = 0, rejected = 0;
+	double last_err = 0, last_dmdt = 0;
+	int not_finite = 0;
+	// host-side copy of the k pointer order (device table is swapped by the controller)
+	void *kh[MAXS] = {};
+	CellArgs<double> args64{};
+	CellArgs<float> args32{};
+};
+
+namespace mm {
+namespace {
+
+inline int grid1(size_t n)
+{
+	const size_t want = (n + 255) / 256;
+	const size_t cap = (size_t)num_sms() * 8;
+	return (int)(want < cap ? (want > 0 ? want : 1) : cap);
+}
+
+template <typename T>
+void fill_args(mm_solver *s, CellArgs<T> &a)
+{
+	const mm_solver_config &c = s->cfg;
+	a.nx = c.nx; a.ny = c.ny; a.nz = c.nz;
+	a.wx = (T)(1.0 / (c.dx * c.dx)); a.wy = (T)(1.0 / (c.dy * c.dy)); a.wz = (T)(1.0 / (c.dz * c.dz));
+	a.idx1 = (T)(1.0 / c.dx); a.idy1 = (T)(1.0 / c.dy); a.idz1 = (T)(1.0 / c.dz);
+	a.idx2 = (T)(1.0 / (2 * c.dx)); a.idy2 = (T)(1.0 / (2 * c.dy)); a.idz2 = (T)(1.0 / (2 * c.dz));
+	a.terms = c.terms;
+	a.reg = s->reg;
+	a.mat = (const DevMat<T> *)s->mat;
+	for (int q = 0; q < 3; ++q) { a.Hext[q] = c.H_ext[q]; a.Hpulse[q] = c.H_pulse[q]; }
+	a.rise = c.pulse_rise;
+}
+
+template <typename T>
+mm_status build_materials(mm_solver *s, int nmat, const mm_material *mats)
+{
+	std::vector<DevMat<T>> h(nmat);
+	std::vector<T> ms(nmat);
+	const mm_solver_config &c = s->cfg;
+	for (int r = 0; r < nmat; ++r) {
+		const mm_material &m = mats[r];
+		DevMat<T> d{};
+		const double Ms = m.Ms;
+		d.Ms = (T)Ms;
+		ms[r] = (T)Ms;
+		if (Ms != 0.0) {
+			d.cex = (T)((2.0 / MU0) * m.A / Ms);
+			// landau_lifshitz_gilbert.py:133-158 factors, scaled to unit m
+			const double gp = GYROMAGNETIC_RATIO / (1.0 + m.alpha * m.alpha);
+			d.l1 = (T)(c.do_precess ? -gp : 0.0);
+			d.l2 = (T)(-m.alpha * gp);
+			d.ku = (T)(2.0 * m.k_uniaxial / Ms / MU0);
+			d.kc = (T)((-2.0 / MU0) * m.k_cubic / Ms);
+			// fdm_zhangli_cpu.cpp:85-101 factors, scaled to unit m and u' = u/Ms
+			const double bj = m.P * MU_BOHR / (ELECTRON_CHARGE * Ms * (1.0 + m.xi * m.xi));
+			const double bjp = bj / (1.0 + m.alpha * m.alpha);
+			const double c1 = c.zl_do_precess ? (1.0 + m.alpha * m.xi) : (m.alpha * m.xi);
+			const double c2 = c.zl_do_precess ? (m.xi - m.alpha) : (-m.alpha);
+			d.zl1 = (T)(-bjp * c1);
+			d.zl2 = (T)(-bjp * c2);
+		}
+		for (int q = 0; q < 3; ++q) {
+			d.a1[q] = (T)m.axis1[q];
+			d.a2[q] = (T)m.axis2[q];
+			d.j[q] = (T)m.j[q];
+		}
+		d.a3[0] = (T)(m.axis1[1] * m.axis2[2] - m.axis1[2] * m.axis2[1]);
+		d.a3[1] = (T)(m.axis1[2] * m.axis2[0] - m.axis1[0] * m.axis2[2]);
+		d.a3[2] = (T)(m.axis1[0] * m.axis2[1] - m.axis1[1] * m.axis2[0]);
+		h[r] = d;
+	}
+	MM_CUDA(cudaMalloc(&s->mat, sizeof(DevMat<T>) * nmat));
+	MM_CUDA(cudaMemcpy(s->mat, h.data(), sizeof(DevMat<T>) * nmat, cudaMemcpyHostToDevice));
+	MM_CUDA(cudaMalloc(&s->ms_tab, sizeof(T) * nmat));
+	MM_CUDA(cudaMemcpy(s->ms_tab, ms.data(), sizeof(T) * nmat, cudaMemcpyHostToDevice));
+	return MM_OK;
+}
+
+template <typename T>
+mm_status alloc_state(mm_solver *s)
+{
+	const size_t b3 = sizeof(T) * 3 * s->n;
+	const bool comp = s->cfg.precision == MM_F32;
+	MM_CUDA(cudaMalloc(&s->m, b3));
+	MM_CUDA(cudaMemset(s->m, 0, b3));
+	if (comp) {
+		MM_CUDA(cudaMalloc(&s->m_lo, b3));
+		MM_CUDA(cudaMemset(s->m_lo, 0, b3));
+		MM_CUDA(cudaMalloc(&s->ynew_lo, b3));
+	}
+	for (int q = 0; q < 2; ++q) MM_CUDA(cudaMalloc(&s->ys[q], b3));
+	for (int q = 0; q < s->tab.s; ++q) {
+		MM_CUDA(cudaMalloc(&s->k[q], b3));
+		MM_CUDA(cudaMemset(s->k[q], 0, b3));
+		s->kh[q] = s->k[q];
+	}
+	MM_CUDA(cudaMalloc(&s->hd, b3));
+	MM_CUDA(cudaMemset(s->hd, 0, b3));
+	KTab<T> kt{};
+	for (int q = 0; q < s->tab.s; ++q) kt.k[q] = (T *)s->k[q];
+	MM_CUDA(cudaMalloc(&s->ktab, sizeof(KTab<T>)));
+	MM_CUDA(cudaMemcpy(s->ktab, &kt, sizeof(kt), cudaMemcpyHostToDevice));
+	MM_CUDA(cudaMalloc(&s->dst, sizeof(DevState)));
+	MM_CUDA(cudaMemset(s->dst, 0, sizeof(DevState)));
+	MM_CUDA(cudaMallocHost(&s->hst, sizeof(DevState)));
+	std::memset(s->hst, 0, sizeof(DevState));
+	MM_CUDA(cudaMalloc(&s->avg, 4 * sizeof(double)));
+	MM_CUDA(cudaMallocHost(&s->avg_h, 4 * sizeof(double)));
+	return MM_OK;
+}
+
+template <typename T>
+const CellArgs<T> &args_of(mm_solver *s);
+template <>
+const CellArgs<double> &args_of<double>(mm_solver *s) { return s->args64; }
+template <>
+const CellArgs<float> &args_of<float>(mm_solver *s) { return s->args32; }
+
+dim3 cell_grid(const mm_solver_config &c) { return dim3((c.nx + 31) / 32, (c.ny + 7) / 8, c.nz); }
+
+// Demag field of the state y (unit, T) into s->hd.
+template <typename T>
+mm_status demag(mm_solver *s, const void *y, cudaStream_t st)
+{
+	if (!(s->cfg.terms & MM_TERM_DEMAG)) return MM_OK;
+	return conv_execute(s->conv, y, s->reg, s->ms_tab, s->hd, st);
+}
+
+
+// y_1 = y_n + h b_10 k_0 when k_0 is the previous attempt's last stage (first same as last).
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_prepare1(size_t n3, double b10, const T *__restrict__ yhi,
+                                                  const T *__restrict__ ylo,
+                                                  const KTab<T> *__restrict__ ktab,
+                                                  const DevState *__restrict__ st, T *__restrict__ y1)
+{
+	const T f = (T)(st->h * b10);
+	const T *k0 = ktab->k[0];
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3; i += (size_t)gridDim.x * blockDim.x) {
+		if (COMP) y1[i] = yhi[i] + (ylo[i] + f * k0[i]);
+		else y1[i] = yhi[i] + f * k0[i];
+	}
+}
+
+// One Runge-Kutta attempt from the current state with the step size and start time already in
+// the device state.  Stage i >= 1 reads y_i from ys[(i-1)&1] and writes y_{i+1} to ys[i&1];
+// the last stage writes y_{n+1} to ys[(s-1)&1] or, for first-same-as-last tableaus in FP64,
+// leaves it as its own input ys[(s-2)&1].
+template <typename T>
+mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
+{
+	constexpr bool COMP = sizeof(T) == 4;
+	const Tableau &tb = s->tab;
+	const CellArgs<T> &a = args_of<T>(s);
+	const dim3 grid = cell_grid(s->cfg), block(32, 8, 1);
+	DevState *ds = s->dst;
+	double *red_err = &ds->max_err2, *red_k0 = &ds->max_k02;
+	const T *yhi = (const T *)s->m, *ylo = (const T *)s->m_lo;
+	const KTab<T> *kt = (const KTab<T> *)s->ktab;
+	T *ys[2] = {(T *)s->ys[0], (T *)s->ys[1]};
+	if (eval_k0) {
+		StageCoef sc{};
+		sc.stage = 0;
+		sc.a_i = tb.a[0];
+		sc.write_next = 1;
+		sc.bn[0] = tb.b[1][0];
+		MM_TRY(demag<T>(s, s->m, st));
+		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yhi, (const T *)s->hd, yhi, ylo, kt, ys[0],
+		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
+		MM_TRY(after_launch("k_stage"));
+	} else {
+		const size_t n3 = 3 * s->n;
+		k_prepare1<T, COMP><<<grid1(n3), 256, 0, st>>>(n3, tb.b[1][0], yhi, ylo, kt, ds, ys[0]);
+		MM_TRY(after_launch("k_prepare1"));
+	}
+	for (int i = 1; i < tb.s; ++i) {
+		StageCoef sc{};
+		sc.stage = i;
+		sc.last = (i == tb.s - 1);
+		sc.a_i = tb.a[i];
+		sc.reduce_k0 = (i == 1);
+		if (!sc.last) {
+			sc.write_next = 1;
+			for (int l = 0; l <= i; ++l) sc.bn[l] = tb.b[i + 1][l];
+		} else {
+			sc.write_new = COMP || !tb.fsal;
+			for (int l = 0; l <= i; ++l) {
+				sc.bn[l] = tb.c[l];
+				sc.ec[l] = tb.ec[l];
+			}
+		}
+		const T *yin = ys[(i - 1) & 1];
+		MM_TRY(demag<T>(s, yin, st));
+		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, ys[i & 1],
+		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
+		MM_TRY(after_launch("k_stage"));
+		if (sc.last) s->last_stage_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
+	}
+	return MM_OK;
+}
+
+template <typename T>
+mm_status controller(mm_solver *s, cudaStream_t st)
+{
+	k_controller<T><<<1, 1, 0, st>>>(s->dst, (KTab<T> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel, s->tab.order,
+	                                 s->tab.fsal, s->tab.s, s->hst);
+	MM_TRY(after_launch("k_controller"));
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+template <typename T>
+mm_status accept_state(mm_solver *s, cudaStream_t st)
+{
+	constexpr bool COMP = sizeof(T) == 4;
+	k_accept<T, COMP><<<grid1(s->n), 256, 0, st>>>(s->n, (const T *)s->ys[s->last_stage_buf],
+	                                                (const T *)s->ynew_lo, (T *)s->m, (T *)s->m_lo);
+	return after_launch("k_accept");
+}
+
+mm_status put_time(mm_solver *s, double t, double h, cudaStream_t st)
+{
+	// the two leading fields of the device state; pinned staging keeps the copy stream-ordered
+	s->hst->t = t;
+	s->hst->h = h;
+	MM_CUDA(cudaMemcpyAsync(s->dst, s->hst, 2 * sizeof(double), cudaMemcpyHostToDevice, st));
+	return MM_OK;
+}
+
+// One attempt + controller; returns the decision in s->hst.
+template <typename T>
+mm_status attempt_and_control(mm_solver *s, double h, cudaStream_t st)
+{
+	MM_TRY(put_time(s, s->t, h, st));
+	const bool eval_k0 = !(s->tab.fsal && s->k0_valid);
+	MM_TRY(attempt<T>(s, eval_k0, st));
+	MM_TRY(controller<T>(s, st));
+	s->attempts++;
+	if (s->tab.fsal) s->k0_valid = true;
+	return MM_OK;
+}
+
+// RungeKutta.evolve(state, t_max) (runge_kutta.py:47-87) + finish_step.
+template <typename T>
+mm_status evolve(mm_solver *s, double t_max, cudaStream_t st)
+{
+	double h_try = s->have_next ? s->h_next : s->h;
+	double h_new = h_try;
+	for (;;) {
+		MM_TRY(attempt_and_control<T>(s, h_try, st));
+		const DevState &d = *s->hst;
+		if (d.not_finite) {
+			s->not_finite = 1;
+			return fail(MM_ERR_NOT_FINITE, "solver: non-finite value in the state or its derivative");
+		}
+		h_new = d.h_new;
+		if (!d.accept) {
+			s->rejected++;
+			if (!s->cfg.fsal_reuse_after_reject) s->k0_valid = false;
+			h_try = h_new;
+			continue;
+		}
+		break;
+	}
+	if (s->t + h_try > t_max) {
+		// runge_kutta.py:75-78: redo the step with the clamped size, accepted without a check
+		h_try = t_max - s->t;
+		MM_TRY(put_time(s, s->t, h_try, st));
+		MM_TRY(attempt<T>(s, !(s->tab.fsal && s->k0_valid), st));
+		MM_TRY(controller<T>(s, st));  // keeps the reductions reset and the FSAL swap in step
+		s->attempts++;
+		if (s->tab.fsal) s->k0_valid = true;
+	}
+	MM_TRY(accept_state<T>(s, st));
+	s->t += h_try;
+	s->h = h_try;
+	s->h_next = h_new;
+	s->have_next = true;
+	s->steps++;
+	return MM_OK;
+}
+
+template <typename T>
+mm_status average(mm_solver *s, double *out3, cudaStream_t st)
+{
+	constexpr bool COMP = sizeof(T) == 4;
+	MM_CUDA(cudaMemsetAsync(s->avg, 0, 3 * sizeof(double), st));
+	k_average_M<T, COMP><<<grid1(s->n), 256, 0, st>>>(s->n, (const T *)s->m, (const T *)s->m_lo, s->reg,
+	                                                   (const DevMat<T> *)s->mat, s->avg);
+	MM_TRY(after_launch("k_average_M"));
+	MM_CUDA(cudaMemcpyAsync(s->avg_h, s->avg, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	for (int c = 0; c < 3; ++c) out3[c] = s->avg_h[c] / (double)s->n;
+	return MM_OK;
+}
+
+void free_solver(mm_solver *s)
+{
+	if (!s) return;
+	delete s->conv;
+	cudaFree(s->mat);
+	cudaFree(s->ms_tab);
+	cudaFree(s->reg);
+	cudaFree(s->m);
+	cudaFree(s->m_lo);
+	cudaFree(s->ys[0]);
+	cudaFree(s->ys[1]);
+	cudaFree(s->ynew_lo);
+	for (int q = 0; q < MAXS; ++q) cudaFree(s->k[q]);
+	cudaFree(s->hd);
+	cudaFree(s->ktab);
+	cudaFree(s->dst);
+	cudaFreeHost(s->hst);
+	cudaFree(s->avg);
+	cudaFreeHost(s->avg_h);
+	delete s;
+}
+
+template <typename T>
+mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uint8_t *regions,
+                      const double *tensor, cudaStream_t st)
+{
+	MM_TRY(build_materials<T>(s, nmat, mats));
+	if (regions) {
+		for (size_t i = 0; i < s->n; ++i)
+			if (regions[i] >= nmat) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: region index out of range");
+		MM_CUDA(cudaMalloc(&s->reg, s->n));
+		MM_CUDA(cudaMemcpy(s->reg, regions, s->n, cudaMemcpyHostToDevice));
+	}
+	MM_TRY(alloc_state<T>(s));
+	fill_args<double>(s, s->args64);
+	fill_args<float>(s, s->args32);
+	if (s->cfg.terms & MM_TERM_DEMAG) {
+		const mm_solver_config &c = s->cfg;
+		double *N = nullptr;
+		const size_t tb = sizeof(double) * 6 * (size_t)s->px * s->py * s->pz;
+		if (!tensor) {
+			MM_CUDA(cudaMalloc(&N, tb));
+			const mm_status r = mm_demag_tensor(c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, s->px, s->py, s->pz, N, st);
+			if (r != MM_OK) { cudaFree(N); return r; }
+		}
+		const mm_status r = conv_plan_create(&s->conv, c.precision, c.nx, c.ny, c.nz, s->px, s->py, s->pz,
+		                                     tensor ? tensor : N, st);
+		if (N) cudaFree(N);
+		MM_TRY(r);
+	}
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+} // namespace
+} // namespace mm
+
+extern "C" {
+
+MM_API mm_status mm_solver_create(mm_solver **out, const mm_solver_config *config, int num_materials,
+                                  const mm_material *materials_host, const uint8_t *regions_host,
+                                  const double *tensor_device, void *stream)
+{
+	if (!out || !config || !materials_host || num_materials <= 0 || num_materials > 256)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid argument");
+	const mm_solver_config &c = *config;
+	if (c.nx <= 0 || c.ny <= 0 || c.nz <= 0 || !(c.dx > 0) || !(c.dy > 0) || !(c.dz > 0))
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid mesh");
+	if (c.precision != MM_F64 && c.precision != MM_F32)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid precision");
+	if (c.tableau < MM_RK_RKF45 || c.tableau > MM_RK_RK23)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid tableau");
+	if (!(c.eps_abs > 0) || !(c.eps_rel > 0) || !(c.h0 > 0))
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: tolerances and h0 must be positive");
+	if ((size_t)c.nx * c.ny * c.nz > (size_t)1 << 31)
+		return fail(MM_ERR_UNSUPPORTED, "mm_solver_create: more than 2^31 cells");
+	mm_solver *s = new mm_solver();
+	s->cfg = c;
+	s->n = (size_t)c.nx * c.ny * c.nz;
+	s->tab = make_tableau(c.tableau);
+	s->px = mm_round_tensor_dimension(c.nx, 0, c.padding);
+	s->py = mm_round_tensor_dimension(c.ny, 0, c.padding);
+	s->pz = mm_round_tensor_dimension(c.nz, 0, c.padding);
+	if (s->px <= 0 || s->py <= 0 || s->pz <= 0) {
+		delete s;
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid padding");
+	}
+	s->h = c.h0;
+	cudaStream_t st = as_stream(stream);
+	const mm_status r = c.precision == MM_F64
+	                        ? create_impl<double>(s, num_materials, materials_host, regions_host, tensor_device, st)
+	                        : create_impl<float>(s, num_materials, materials_host, regions_host, tensor_device, st);
+	if (r != MM_OK) {
+		free_solver(s);
+		return r;
+	}
+	*out = s;
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_destroy(mm_solver *s)
+{
+	free_solver(s);
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_set_M(mm_solver *s, const double *M, void *stream)
+{
+	if (!s || !M) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_set_M: null argument");
+	cudaStream_t st = as_stream(stream);
+	if (s->cfg.precision == MM_F64)
+		k_set_M<double, false><<<grid1(s->n), 256, 0, st>>>(s->n, M, s->reg, (const DevMat<double> *)s->mat,
+		                                                     (double *)s->m, nullptr);
+	else
+		k_set_M<float, true><<<grid1(s->n), 256, 0, st>>>(s->n, M, s->reg, (const DevMat<float> *)s->mat,
+		                                                   (float *)s->m, (float *)s->m_lo);
+	MM_TRY(after_launch("k_set_M"));
+	s->t = 0;
+	s->h = s->cfg.h0;
+	s->have_next = false;
+	s->k0_valid = false;
+	s->steps = s->attempts = s->rejected = 0;
+	s->not_finite = 0;
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_get_M(mm_solver *s, double *M, void *stream)
+{
+	if (!s || !M) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_get_M: null argument");
+	cudaStream_t st = as_stream(stream);
+	if (s->cfg.precision == MM_F64)
+		k_get_M<double, false><<<grid1(s->n), 256, 0, st>>>(s->n, (const double *)s->m, nullptr, s->reg,
+		                                                     (const DevMat<double> *)s->mat, M);
+	else
+		k_get_M<float, true><<<grid1(s->n), 256, 0, st>>>(s->n, (const float *)s->m, (const float *)s->m_lo,
+		                                                   s->reg, (const DevMat<float> *)s->mat, M);
+	return after_launch("k_get_M");
+}
+
+MM_API mm_status mm_solver_set_time(mm_solver *s, double t, double h_next, void *stream)
+{
+	(void)stream;
+	if (!s || !(h_next > 0)) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_set_time: invalid argument");
+	s->t = t;
+	s->h_next = h_next;
+	s->have_next = true;
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_step(mm_solver *s, double t_max, void *stream)
+{
+	if (!s) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_step: null solver");
+	cudaStream_t st = as_stream(stream);
+	MM_TRY(s->cfg.precision == MM_F64 ? evolve<double>(s, t_max, st) : evolve<float>(s, t_max, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_run(mm_solver *s, double t_end, double sample_dt, double *sample_t_host,
+                               double *samples_host, int max_samples, int *num_samples, void *stream)
+{
+	if (!s) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_run: null solver");
+	cudaStream_t st = as_stream(stream);
+	const bool sampling = sample_dt > 0 && samples_host && sample_t_host;
+	int count = 0;
+	auto handle = [&]() -> mm_status {
+		// condition.EveryNthSecond.check (condition.py:121-133)
+		if (!sampling) return MM_OK;
+		const double r = fmod(s->t, sample_dt);
+		if ((fabs(r) < 1e-16 || fabs(r - sample_dt) < 1e-16) && count < max_samples) {
+			sample_t_host[count] = s->t;
+			MM_TRY(s->cfg.precision == MM_F64 ? average<double>(s, samples_host + 3 * count, st)
+			                                  : average<float>(s, samples_host + 3 * count, st));
+			++count;
+		}
+		return MM_OK;
+	};
+	MM_TRY(handle());
+	while (!(s->t >= t_end)) {
+		// Solver.step_with_t_max (solver.py:76-85): the next time of interest of the handlers
+		double t1 = 1e100;
+		if (sampling) {
+			const double toi = ((double)(long long)(s->t / sample_dt) + 1) * sample_dt;
+			if (toi > s->t && toi < t1) t1 = toi;
+		}
+		MM_TRY(s->cfg.precision == MM_F64 ? evolve<double>(s, t1, st) : evolve<float>(s, t1, st));
+		MM_TRY(handle());
+	}
+	if (num_samples) *num_samples = count;
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_attempt(mm_solver *s, double h, void *stream)
+{
+	if (!s || !(h > 0)) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_attempt: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	MM_TRY(put_time(s, s->t, h, st));
+	const bool eval_k0 = !(s->tab.fsal && s->k0_valid);
+	if (s->cfg.precision == MM_F64) {
+		MM_TRY(attempt<double>(s, eval_k0, st));
+		k_controller<double><<<1, 1, 0, st>>>(s->dst, (KTab<double> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
+		                                      s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+	} else {
+		MM_TRY(attempt<float>(s, eval_k0, st));
+		k_controller<float><<<1, 1, 0, st>>>(s->dst, (KTab<float> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
+		                                     s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+	}
+	MM_TRY(after_launch("k_controller"));
+	if (s->tab.fsal) s->k0_valid = true;
+	s->attempts++;
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_eval(mm_solver *s, double *H_eff, double *dMdt, double *H_demag, void *stream)
+{
+	if (!s) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_eval: null solver");
+	cudaStream_t st = as_stream(stream);
+	const dim3 grid = cell_grid(s->cfg), block(32, 8, 1);
+	if (s->cfg.precision == MM_F64) {
+		MM_TRY(demag<double>(s, s->m, st));
+		k_eval<double><<<grid, block, 0, st>>>(s->args64, (const double *)s->m, (const double *)s->hd, s->t, H_eff,
+		                                       dMdt, H_demag);
+	} else {
+		MM_TRY(demag<float>(s, s->m, st));
+		k_eval<float><<<grid, block, 0, st>>>(s->args32, (const float *)s->m, (const float *)s->hd, s->t, H_eff,
+		                                      dMdt, H_demag);
+	}
+	return after_launch("k_eval");
+}
+
+MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *stream)
+{
+	(void)stream;
+	if (!s || !out) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_stats_get: null argument");
+	out->t = s->t;
+	out->h = s->h;
+	out->h_next = s->have_next ? s->h_next : s->h;
+	out->steps = s->steps;
+	out->attempts = s->attempts;
+	out->rejected = s->rejected;
+	out->last_error = sqrt(s->hst->max_err2);
+	out->last_max_dmdt = sqrt(s->hst->max_k02);
+	out->not_finite = s->not_finite;
+	return MM_OK;
+}
+
+MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg3, void *stream)
+{
+	if (!s || !avg3) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_average_M: null argument");
+	cudaStream_t st = as_stream(stream);
+	return s->cfg.precision == MM_F64 ? average<double>(s, avg3, st) : average<float>(s, avg3, st);
+}
+
+} // extern "C"

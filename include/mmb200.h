@@ -59,6 +59,17 @@ MM_API int mm_abi_version(void);
 /* Number of kernels this library has launched in the process (for launch accounting). */
 MM_API uint64_t mm_kernel_launch_count(void);
 
+/* Per-kernel timing of the solver and convolution kernels (no counterpart in the reference,
+ * whose --prof switch times host sections, Benchmark.cpp:53-109).  When enabled, each launch is
+ * bracketed by CUDA events on its stream; mm_profile_get() synchronises and returns, per kernel
+ * name, the launch count, the summed device time and the summed algorithmic bytes (each array
+ * element crossing HBM once per launch).  Not thread-safe across concurrent solvers. */
+MM_API mm_status mm_profile_enable(int on);
+MM_API mm_status mm_profile_reset(void);
+MM_API int mm_profile_count(void);
+MM_API mm_status mm_profile_get(int index, const char **name, int64_t *launches, double *total_ms,
+                                double *bytes);
+
 /* ---------------------------------------------------------------------------------------------
  * Field terms: one call per term, same arguments and results as the reference's magneto calls.
  * ------------------------------------------------------------------------------------------- */
@@ -231,6 +242,9 @@ MM_API mm_status mm_solver_destroy(mm_solver *s);
  * step counters, and forgets the first-same-as-last stage. */
 MM_API mm_status mm_solver_set_M(mm_solver *s, const double *M_device, void *stream);
 MM_API mm_status mm_solver_get_M(mm_solver *s, double *M_device, void *stream);
+/* Replace the state by M (normalised to Ms) keeping t, the step size, the counters and the
+ * first-same-as-last stage: for callers that keep M in their own buffers between steps. */
+MM_API mm_status mm_solver_load_M(mm_solver *s, const double *M_device, void *stream);
 MM_API mm_status mm_solver_set_time(mm_solver *s, double t, double h_next, void *stream);
 
 /* One accepted step toward t_max: RungeKutta.evolve(state, t_max) (runge_kutta.py:47-87)

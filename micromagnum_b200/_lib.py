@@ -68,6 +68,10 @@ _PROTOS = [
     ("mm_last_error", ctypes.c_char_p, []),
     ("mm_abi_version", _I, []),
     ("mm_kernel_launch_count", ctypes.c_uint64, []),
+    ("mm_profile_enable", _I, [_I]),
+    ("mm_profile_reset", _I, []),
+    ("mm_profile_count", _I, []),
+    ("mm_profile_get", _I, [_I, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(ctypes.c_int64), _DP, _DP]),
     ("mm_exchange", _I, [_I, _I, _I, _I, _D, _D, _D, _I, _I, _I, _VP, _VP, _VP, _VP, _DP, _VP]),
     ("mm_uniaxial_anisotropy", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _DP, _VP]),
     ("mm_cubic_anisotropy", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _VP, _DP, _VP]),
@@ -87,6 +91,7 @@ _PROTOS = [
     ("mm_solver_destroy", _I, [_VP]),
     ("mm_solver_set_M", _I, [_VP, _VP, _VP]),
     ("mm_solver_get_M", _I, [_VP, _VP, _VP]),
+    ("mm_solver_load_M", _I, [_VP, _VP, _VP]),
     ("mm_solver_set_time", _I, [_VP, _D, _D, _VP]),
     ("mm_solver_step", _I, [_VP, _D, _VP]),
     ("mm_solver_run", _I, [_VP, _D, _D, _DP, _DP, _I, ctypes.POINTER(_I), _VP]),
@@ -133,3 +138,24 @@ def check(status: int) -> None:
 
 def launches() -> int:
     return int(lib().mm_kernel_launch_count())
+
+
+def profile_enable(on: bool = True) -> None:
+    check(lib().mm_profile_enable(int(on)))
+
+
+def profile_reset() -> None:
+    check(lib().mm_profile_reset())
+
+
+def profile_read() -> dict:
+    """{kernel name: (launches, total device ms, total algorithmic bytes)} (synchronises)."""
+    out = {}
+    for i in range(lib().mm_profile_count()):
+        name = ctypes.c_char_p()
+        cnt = ctypes.c_int64()
+        ms = ctypes.c_double()
+        by = ctypes.c_double()
+        check(lib().mm_profile_get(i, ctypes.byref(name), ctypes.byref(cnt), ctypes.byref(ms), ctypes.byref(by)))
+        out[name.value.decode()] = (cnt.value, ms.value, by.value)
+    return out

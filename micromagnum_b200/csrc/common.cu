@@ -44,9 +44,122 @@ mm_status scalar_scratch(ScalarScratch **out)
 	return MM_OK;
 }
 
+// ---- profiler ------------------------------------------------------------------------------------
+namespace {
+struct ProfRecord {
+	std::string name;
+	double bytes;
+	cudaEvent_t start, stop;
+};
+struct ProfTotals {
+	std::string name;
+	int64_t launches = 0;
+	double total_ms = 0.0;
+	double bytes = 0.0;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRecord> g_prof_pending;
+std::vector<ProfTotals> g_prof_totals;
+std::vector<cudaEvent_t> g_event_pool;
+
+cudaEvent_t take_event()
+{
+	if (!g_event_pool.empty()) {
+		cudaEvent_t e = g_event_pool.back();
+		g_event_pool.pop_back();
+		return e;
+	}
+	cudaEvent_t e = nullptr;
+	cudaEventCreate(&e);
+	return e;
+}
+
+void drain_pending()
+{
+	for (ProfRecord &r : g_prof_pending) {
+		float ms = 0.f;
+		cudaEventSynchronize(r.stop);
+		cudaEventElapsedTime(&ms, r.start, r.stop);
+		ProfTotals *t = nullptr;
+		for (ProfTotals &x : g_prof_totals)
+			if (x.name == r.name) t = &x;
+		if (!t) {
+			g_prof_totals.push_back(ProfTotals{r.name});
+			t = &g_prof_totals.back();
+		}
+		t->launches++;
+		t->total_ms += ms;
+		t->bytes += r.bytes;
+		g_event_pool.push_back(r.start);
+		g_event_pool.push_back(r.stop);
+	}
+	g_prof_pending.clear();
+}
+} // namespace
+
+bool profiling_on() { return g_prof_on; }
+
+ProfToken prof_begin(cudaStream_t st)
+{
+	ProfToken t;
+	if (!g_prof_on) return t;
+	std::lock_guard<std::mutex> lock(g_prof_mu);
+	t.start = take_event();
+	cudaEventRecord(t.start, st);
+	return t;
+}
+
+void prof_end(ProfToken tok, const char *name, double bytes, cudaStream_t st)
+{
+	if (!g_prof_on || !tok.start) return;
+	std::lock_guard<std::mutex> lock(g_prof_mu);
+	cudaEvent_t stop = take_event();
+	cudaEventRecord(stop, st);
+	g_prof_pending.push_back(ProfRecord{name, bytes, tok.start, stop});
+	if (g_prof_pending.size() > 4096) drain_pending();
+}
+
 } // namespace mm
 
 extern "C" {
+
+MM_API mm_status mm_profile_enable(int on)
+{
+	std::lock_guard<std::mutex> lock(mm::g_prof_mu);
+	mm::g_prof_on = on != 0;
+	return MM_OK;
+}
+
+MM_API mm_status mm_profile_reset(void)
+{
+	std::lock_guard<std::mutex> lock(mm::g_prof_mu);
+	mm::drain_pending();
+	mm::g_prof_totals.clear();
+	return MM_OK;
+}
+
+MM_API int mm_profile_count(void)
+{
+	std::lock_guard<std::mutex> lock(mm::g_prof_mu);
+	mm::drain_pending();
+	return (int)mm::g_prof_totals.size();
+}
+
+MM_API mm_status mm_profile_get(int index, const char **name, int64_t *launches, double *total_ms,
+                                double *bytes)
+{
+	std::lock_guard<std::mutex> lock(mm::g_prof_mu);
+	mm::drain_pending();
+	if (index < 0 || index >= (int)mm::g_prof_totals.size())
+		return mm::fail(MM_ERR_INVALID_ARGUMENT, "mm_profile_get: index out of range");
+	const auto &t = mm::g_prof_totals[index];
+	if (name) *name = t.name.c_str();
+	if (launches) *launches = t.launches;
+	if (total_ms) *total_ms = t.total_ms;
+	if (bytes) *bytes = t.bytes;
+	return MM_OK;
+}
 
 MM_API const char *mm_last_error(void) { return mm::g_last_error.c_str(); }
 MM_API int mm_abi_version(void) { return MM_ABI_VERSION; }

@@ -493,6 +493,12 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	const int rows = 3 * p->ny * p->nz;
 	const int lines = (rows + 1) / 2;
 	const int gx = (lines + p->lp_x - 1) / p->lp_x;
+	// algorithmic bytes of each pass (every array element crossing HBM once)
+	const double n = (double)p->nx * p->ny * p->nz, s = sizeof(T), c = sizeof(C);
+	const double half = 3.0 * p->hx * p->ny * p->nz * c;      // x-transformed rows y < ny, z < nz
+	const double ypad = 3.0 * p->hx * p->py * p->nz * c;      // y-transformed, z < nz
+	const double tens = 6.0 * p->hx * p->qy * p->qz * s;
+	ProfToken tk = prof_begin(st);
 	if (ms_tab)
 		k_x_fwd<T, true><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
 		                                            p->rx, (const C *)p->tw_x, p->lp_x);
@@ -500,27 +506,39 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		k_x_fwd<T, false><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
 		                                             p->rx, (const C *)p->tw_x, p->lp_x);
 	MM_TRY(after_launch("k_x_fwd"));
+	prof_end(tk, "k_x_fwd", 3 * n * s + (reg ? n : 0.0) + half, st);
 	if (p->is2d) {
 		const int gy = (p->hx + p->tb_y - 1) / p->tb_y;
+		tk = prof_begin(st);
 		k_y_mul2d<T><<<gy, NT, p->smem_y, st>>>(S, (const T *)p->tensor, p->ny, p->hx, p->qy, p->ry,
 		                                        (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_mul2d"));
+		prof_end(tk, "k_y_mul2d", 2 * half + tens, st);
 	} else {
 		dim3 gy((p->hx + p->tb_y - 1) / p->tb_y, p->nz, 3);
+		tk = prof_begin(st);
 		k_y<T, false><<<gy, NT, p->smem_y, st>>>(S, p->ny, p->py, p->nz, p->py, p->hx, p->ry,
 		                                         (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_fwd"));
+		prof_end(tk, "k_y_fwd", half + ypad, st);
 		dim3 gz((p->hx + p->tb_z - 1) / p->tb_z, p->py, 1);
+		tk = prof_begin(st);
 		k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz,
 		                                      p->rz, (const C *)p->tw_z, p->tb_z);
 		MM_TRY(after_launch("k_z_mul"));
+		prof_end(tk, "k_z_mul", 2 * ypad + tens, st);
+		tk = prof_begin(st);
 		k_y<T, true><<<gy, NT, p->smem_y, st>>>(S, p->py, p->ny, p->nz, p->py, p->hx, p->ry,
 		                                        (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_inv"));
+		prof_end(tk, "k_y_inv", half + ypad, st);
 	}
+	tk = prof_begin(st);
 	k_x_inv<T><<<gx, NT, p->smem_x, st>>>(S, H, p->nx, p->ny, p->nz, p->py, p->hx, p->rx,
 	                                      (const C *)p->tw_x, p->lp_x);
-	return after_launch("k_x_inv");
+	MM_TRY(after_launch("k_x_inv"));
+	prof_end(tk, "k_x_inv", half + 3 * n * s, st);
+	return MM_OK;
 }
 
 } // namespace

@@ -54,6 +54,14 @@ inline mm_status after_launch(const char *what)
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// ---- optional per-kernel timing (mm_profile_*): CUDA events around solver/convolution launches --
+struct ProfToken {
+	cudaEvent_t start = nullptr;
+};
+bool profiling_on();
+ProfToken prof_begin(cudaStream_t st);
+void prof_end(ProfToken tok, const char *name, double bytes, cudaStream_t st);
+
 // ---- number of SMs of the current device (grid sizing) -------------------------------------------
 int num_sms();
 

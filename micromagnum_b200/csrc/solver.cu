@@ -622,6 +622,28 @@ mm_status demag(mm_solver *s, const void *y, cudaStream_t st)
 }
 
 
+// Algorithmic bytes of one fused stage launch: stencil input, demag field, region ids, the step
+// base, the earlier stages with nonzero weights, and the outputs.
+template <typename T>
+double stage_bytes(const mm_solver *s, const StageCoef &sc)
+{
+	const bool comp = sizeof(T) == 4;
+	const double v = 3.0 * (double)s->n * sizeof(T);
+	double b = v;                                               // y_in
+	if (s->cfg.terms & MM_TERM_DEMAG) b += v;                    // H_demag
+	if (s->reg) b += (double)s->n;                               // region ids
+	b += v;                                                      // k_i written
+	const bool out = sc.last ? sc.write_new : sc.write_next;
+	if (out) {
+		b += v * (comp ? 2 : 1);                                 // y_n (hi, lo)
+		b += v * (comp && sc.last ? 2 : 1);                      // y_out (+ lo)
+	}
+	for (int l = 0; l < sc.stage; ++l)
+		if (sc.bn[l] != 0.0 || (sc.last && sc.ec[l] != 0.0)) b += v;
+	if (sc.reduce_k0 && sc.stage > 0 && sc.bn[0] == 0.0) b += v;
+	return b;
+}
+
 // y_1 = y_n + h b_10 k_0 when k_0 is the previous attempt's last stage (first same as last).
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(256) k_prepare1(size_t n3, double b10, const T *__restrict__ yhi,
@@ -660,13 +682,17 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		sc.write_next = 1;
 		sc.bn[0] = tb.b[1][0];
 		MM_TRY(demag<T>(s, s->m, st));
+		ProfToken tk = prof_begin(st);
 		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yhi, (const T *)s->hd, yhi, ylo, kt, ys[0],
 		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
 		MM_TRY(after_launch("k_stage"));
+		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
 	} else {
 		const size_t n3 = 3 * s->n;
+		ProfToken tk = prof_begin(st);
 		k_prepare1<T, COMP><<<grid1(n3), 256, 0, st>>>(n3, tb.b[1][0], yhi, ylo, kt, ds, ys[0]);
 		MM_TRY(after_launch("k_prepare1"));
+		prof_end(tk, "k_prepare1", (double)n3 * sizeof(T) * (COMP ? 4 : 3), st);
 	}
 	for (int i = 1; i < tb.s; ++i) {
 		StageCoef sc{};
@@ -686,9 +712,11 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		}
 		const T *yin = ys[(i - 1) & 1];
 		MM_TRY(demag<T>(s, yin, st));
+		ProfToken tk = prof_begin(st);
 		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, ys[i & 1],
 		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
 		MM_TRY(after_launch("k_stage"));
+		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
 		if (sc.last) s->last_stage_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
 	}
 	return MM_OK;
@@ -708,9 +736,12 @@ template <typename T>
 mm_status accept_state(mm_solver *s, cudaStream_t st)
 {
 	constexpr bool COMP = sizeof(T) == 4;
+	ProfToken tk = prof_begin(st);
 	k_accept<T, COMP><<<grid1(s->n), 256, 0, st>>>(s->n, (const T *)s->ys[s->last_stage_buf],
 	                                                (const T *)s->ynew_lo, (T *)s->m, (T *)s->m_lo);
-	return after_launch("k_accept");
+	MM_TRY(after_launch("k_accept"));
+	prof_end(tk, "k_accept", 3.0 * s->n * sizeof(T) * (COMP ? 4 : 2), st);
+	return MM_OK;
 }
 
 mm_status put_time(mm_solver *s, double t, double h, cudaStream_t st)
@@ -913,6 +944,19 @@ MM_API mm_status mm_solver_set_M(mm_solver *s, const double *M, void *stream)
 	s->steps = s->attempts = s->rejected = 0;
 	s->not_finite = 0;
 	return MM_OK;
+}
+
+MM_API mm_status mm_solver_load_M(mm_solver *s, const double *M, void *stream)
+{
+	if (!s || !M) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_load_M: null argument");
+	cudaStream_t st = as_stream(stream);
+	if (s->cfg.precision == MM_F64)
+		k_set_M<double, false><<<grid1(s->n), 256, 0, st>>>(s->n, M, s->reg, (const DevMat<double> *)s->mat,
+		                                                     (double *)s->m, nullptr);
+	else
+		k_set_M<float, true><<<grid1(s->n), 256, 0, st>>>(s->n, M, s->reg, (const DevMat<float> *)s->mat,
+		                                                   (float *)s->m, (float *)s->m_lo);
+	return after_launch("k_set_M");
 }
 
 MM_API mm_status mm_solver_get_M(mm_solver *s, double *M, void *stream)

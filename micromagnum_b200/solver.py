@@ -160,6 +160,15 @@ class Solver:
         check(lib().mm_solver_set_M(self._h, ctypes.c_void_p(v.data_ptr()), _stream_ptr()))
         torch.cuda.current_stream().synchronize()
 
+    def load_M_device(self, M_device: torch.Tensor) -> None:
+        """Replace the state by M (a 3N float64 CUDA tensor, A/m) without resetting time, step
+        size or counters (stream-ordered)."""
+        check(lib().mm_solver_load_M(self._h, ctypes.c_void_p(M_device.data_ptr()), _stream_ptr()))
+
+    def read_M_device(self, out: torch.Tensor) -> None:
+        """Write M (A/m) into a 3N float64 CUDA tensor (stream-ordered)."""
+        check(lib().mm_solver_get_M(self._h, ctypes.c_void_p(out.data_ptr()), _stream_ptr()))
+
     def set_time(self, t: float, h_next: float) -> None:
         check(lib().mm_solver_set_time(self._h, t, h_next, _stream_ptr()))
 

@@ -497,20 +497,34 @@ static void fft3(cpx *d, const int L[3], int sign)
 	}
 }
 
-/* math/conv/MatrixVectorConvolution_FFT.cpp:110-241 (CPU path) with the tensor set-up of
- * TensorFieldSetup.cpp:35-74: forward transforms of the padded M, multiplication by the
- * transformed tensor scaled by 1/(ex ey ez) (cpu_multiplication.cpp:56-91), inverse transform,
- * crop. */
-void or_conv_fft(const double *N, int nx, int ny, int nz, int ex, int ey, int ez, const double *M, double *H)
+/* TensorFieldSetup.cpp:35-74: transformed tensor components (full complex spectra). */
+static cpx **conv_fft_prepare(const double *N, int ex, int ey, int ez)
 {
-	const size_t P = (size_t)ex * ey * ez, n = (size_t)nx * ny * nz;
+	const size_t P = (size_t)ex * ey * ez;
 	const int L[3] = {ex, ey, ez};
-	cpx *Nh[6];
+	cpx **Nh = (cpx **)malloc(6 * sizeof(cpx *));
 	for (int c = 0; c < 6; ++c) {
 		Nh[c] = (cpx *)malloc(sizeof(cpx) * P);
 		for (size_t i = 0; i < P; ++i) Nh[c][i] = (cpx){N[6 * i + c], 0.0};
 		fft3(Nh[c], L, -1);
 	}
+	return Nh;
+}
+
+static void conv_fft_free(cpx **Nh)
+{
+	if (!Nh) return;
+	for (int c = 0; c < 6; ++c) free(Nh[c]);
+	free(Nh);
+}
+
+/* math/conv/MatrixVectorConvolution_FFT.cpp:110-241 (CPU path): forward transforms of the padded
+ * M, multiplication by the transformed tensor scaled by 1/(ex ey ez) (cpu_multiplication.cpp:
+ * 56-91), inverse transform, crop. */
+static void conv_fft_apply(cpx **Nh, int nx, int ny, int nz, int ex, int ey, int ez, const double *M, double *H)
+{
+	const size_t P = (size_t)ex * ey * ez, n = (size_t)nx * ny * nz;
+	const int L[3] = {ex, ey, ez};
 	cpx *Mh[3];
 	for (int c = 0; c < 3; ++c) {
 		Mh[c] = (cpx *)calloc(P, sizeof(cpx));
@@ -541,7 +555,13 @@ void or_conv_fft(const double *N, int nx, int ny, int nz, int ex, int ey, int ez
 					H[c * n + ((size_t)z * ny + y) * nx + x] = Mh[c][((size_t)z * ey + y) * ex + x].re;
 		free(Mh[c]);
 	}
-	for (int c = 0; c < 6; ++c) free(Nh[c]);
+}
+
+void or_conv_fft(const double *N, int nx, int ny, int nz, int ex, int ey, int ez, const double *M, double *H)
+{
+	cpx **Nh = conv_fft_prepare(N, ex, ey, ez);
+	conv_fft_apply(Nh, nx, ny, nz, ex, ey, ez, M, H);
+	conv_fft_free(Nh);
 }
 
 /* ------------------------------------------------------------------------------------------ */
@@ -627,6 +647,7 @@ struct or_solver {
 	int ex, ey, ez;
 	double *Ms, *A, *alpha, *kuni, *kcub, *ax1, *ax2, *P, *xi, *j, *N;
 	double *f1, *f2;
+	cpx **Nh;             /* tensor spectrum (FFT convolution) */
 	double *y, *y0, *ytmp, *yerr, *k[8], *Htmp, *Hacc, *dtmp;
 	int k0_is_fsal;       /* state.dydt_in available (held in k[0]) */
 	tableau_t tab;
@@ -656,6 +677,7 @@ or_solver *or_solver_create(const or_solver_config *cfg, const double *Ms, const
 	s->ax1 = dup(axis1, 3 * n); s->ax2 = dup(axis2, 3 * n);
 	s->P = dup(P, n); s->xi = dup(xi, n); s->j = dup(j, 3 * n);
 	s->N = tensor ? dup(tensor, 6 * (size_t)ex * ey * ez) : NULL;
+	s->Nh = (tensor && cfg->use_fft) ? conv_fft_prepare(s->N, ex, ey, ez) : NULL;
 	/* LandauLifshitzGilbert.__initFactors (landau_lifshitz_gilbert.py:133-158) */
 	s->f1 = dup(NULL, n); s->f2 = dup(NULL, n);
 	for (size_t i = 0; i < n; ++i) {
@@ -681,6 +703,7 @@ void or_solver_destroy(or_solver *s)
 	                  s->f1, s->f2, s->y, s->y0, s->ytmp, s->yerr, s->Htmp, s->Hacc, s->dtmp};
 	for (size_t q = 0; q < sizeof(bufs) / sizeof(bufs[0]); ++q) free(bufs[q]);
 	for (int q = 0; q < 8; ++q) free(s->k[q]);
+	conv_fft_free(s->Nh);
 	free(s);
 }
 
@@ -708,7 +731,7 @@ static void rhs(or_solver *s, const double *M, double t, double *dMdt, double *H
 	double *H = Heff ? Heff : s->Hacc;
 	memset(H, 0, sizeof(double) * n3);
 	if (c->terms & 1) {
-		if (c->use_fft) or_conv_fft(s->N, c->nx, c->ny, c->nz, s->ex, s->ey, s->ez, M, s->Htmp);
+		if (c->use_fft) conv_fft_apply(s->Nh, c->nx, c->ny, c->nz, s->ex, s->ey, s->ez, M, s->Htmp);
 		else or_conv_direct(s->N, c->nx, c->ny, c->nz, s->ex, s->ey, s->ez, M, s->Htmp);
 		if (Hdemag) memcpy(Hdemag, s->Htmp, sizeof(double) * n3);
 		add_to(H, s->Htmp, n3);

@@ -352,9 +352,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--dims", default=None, help="override the grid, e.g. 512,512,8 (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.dims:
+        global DIMS, WORKLOAD
+        DIMS = tuple(int(v) for v in args.dims.split(","))
+        WORKLOAD = WORKLOAD.replace("512x512x16", "x".join(map(str, DIMS)))
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -107,11 +107,18 @@ __device__ __forceinline__ void atomic_max_nonneg(double *addr, double v)
 	          static_cast<unsigned long long>(__double_as_longlong(v)));
 }
 
+// max that propagates NaN (fmax would drop it and hide a diverged state from the controller)
+template <typename T>
+__device__ __forceinline__ T nan_max(T a, T b)
+{
+	return (a > b || a != a) ? a : b;
+}
+
 template <typename T>
 __device__ __forceinline__ T warp_max(T v)
 {
 #pragma unroll
-	for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+	for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(0xffffffffu, v, o));
 	return v;
 }
 template <typename T>
@@ -122,19 +129,25 @@ __device__ __forceinline__ T warp_sum(T v)
 	return v;
 }
 
-// Block-wide max of a non-negative value, result atomically folded into *out (double).
-// blockDim.x must be a multiple of 32 and at most 1024.
+__device__ __forceinline__ int block_tid()
+{
+	return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
+
+// Block-wide max of a non-negative value (NaN wins), folded atomically into *out (double).
+// Works for 1-D to 3-D blocks whose thread count is a multiple of 32 (at most 1024).
 template <typename T>
 __device__ __forceinline__ void block_max_to(double *out, T v)
 {
 	__shared__ T red[32];
 	__syncthreads();  // red[] may still be read by a previous reduction in this block
 	v = warp_max(v);
-	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	const int tid = block_tid(), lane = tid & 31, wid = tid >> 5;
 	if (lane == 0) red[wid] = v;
 	__syncthreads();
 	if (wid == 0) {
-		const int nw = blockDim.x >> 5;
+		const int nw = block_threads() >> 5;
 		T w = lane < nw ? red[lane] : T(0);
 		w = warp_max(w);
 		if (lane == 0) atomic_max_nonneg(out, (double)w);
@@ -147,11 +160,11 @@ __device__ __forceinline__ void block_sum_to(double *out, double v)
 	__shared__ double red[32];
 	__syncthreads();
 	v = warp_sum(v);
-	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	const int tid = block_tid(), lane = tid & 31, wid = tid >> 5;
 	if (lane == 0) red[wid] = v;
 	__syncthreads();
 	if (wid == 0) {
-		const int nw = blockDim.x >> 5;
+		const int nw = block_threads() >> 5;
 		double w = lane < nw ? red[lane] : 0.0;
 		w = warp_sum(w);
 		if (lane == 0) atomicAdd(out, w);

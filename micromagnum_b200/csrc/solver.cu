@@ -166,8 +166,16 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
                                          V3<T> &Heff, V3<T> &dm)
 {
 	const DevMat<T> &M = mat_of(a, i);
+	double f = 1.0;
+	if ((a.terms & MM_TERM_ZEEMAN) && a.rise > 0) f = t / a.rise < 1.0 ? t / a.rise : 1.0;
+	const V3<T> Hz = (a.terms & MM_TERM_ZEEMAN)
+	                     ? v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
+	                             (T)(a.Hext[2] + a.Hpulse[2] * f))
+	                     : v3<T>(0, 0, 0);
 	if (M.Ms == T(0)) {
-		Heff = v3<T>(0, 0, 0);
+		// empty cell: no magnetisation and no torque, but the stray and applied fields exist
+		// there (H_tot is the sum of the terms, each zero except these two)
+		Heff = ((a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0)) + Hz;
 		dm = v3<T>(0, 0, 0);
 		return false;
 	}
@@ -205,12 +213,7 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 		const T s1 = p1 * p1, s2 = p2 * p2, s3 = p3 * p3;
 		H = H + M.kc * (((s2 + s3) * p1) * u1 + ((s1 + s3) * p2) * u2 + ((s1 + s2) * p3) * u3);
 	}
-	if (a.terms & MM_TERM_ZEEMAN) {
-		double f = 1.0;
-		if (a.rise > 0) f = t / a.rise < 1.0 ? t / a.rise : 1.0;
-		H = H + v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
-		              (T)(a.Hext[2] + a.Hpulse[2] * f));
-	}
+	H = H + Hz;
 	Heff = H;
 	// llge_cpu.cpp:25-45 on unit m
 	const V3<T> mxh = cross(m, H);

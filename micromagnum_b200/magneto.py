@@ -77,6 +77,13 @@ def _work(t: torch.Tensor) -> torch.Tensor:
     return t.contiguous() if _mode == CUDA_64 else t.to(torch.float32).contiguous()
 
 
+def _works(*fields):
+    """Working-precision tensors of the given containers; the caller keeps the returned list
+    alive until the library call has been issued (a temporary that is released early would let
+    the allocator hand its memory to the next temporary)."""
+    return [_work(f.data) for f in fields]
+
+
 def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -217,7 +224,8 @@ class VectorMatrix(_Base):
             check(lib().mm_normalize(_lib.MM_F64, self._n, _ptr(ms), _ptr(self.data), _stream()))
         else:
             w = _work(self.data)
-            check(lib().mm_normalize(_lib.MM_F32, self._n, _ptr(_work(ms)), _ptr(w), _stream()))
+            msw = _work(ms)
+            check(lib().mm_normalize(_lib.MM_F32, self._n, _ptr(msw), _ptr(w), _stream()))
             self.data.copy_(w)
 
     def absMax(self) -> float:
@@ -263,9 +271,9 @@ def exchange(*args) -> float:
         nx, ny, nz, dx, dy, dz, px, py, pz, Ms, A, M, H = args
     e = ctypes.c_double(0.0)
     out = _work(H.data) if _mode == CUDA_32 else H.data
+    ms, a, m = _works(Ms, A, M)  # working-precision copies live until the call returns
     check(lib().mm_exchange(_prec(), nx, ny, nz, dx, dy, dz, int(px), int(py), int(pz),
-                            _ptr(_work(Ms.data)), _ptr(_work(A.data)), _ptr(_work(M.data)),
-                            _ptr(out), ctypes.byref(e), _stream()))
+                            _ptr(ms), _ptr(a), _ptr(m), _ptr(out), ctypes.byref(e), _stream()))
     if out is not H.data:
         H.data.copy_(out)
     return e.value
@@ -275,8 +283,8 @@ def uniaxial_anisotropy(axis, k, Ms, M, H) -> float:
     """bindings/mmm/anisotropy.i:24-31; returns sum_i k |a x m|^2 (CPU path's value)."""
     e = ctypes.c_double(0.0)
     out = _work(H.data) if _mode == CUDA_32 else H.data
-    check(lib().mm_uniaxial_anisotropy(_prec(), M.size(), _ptr(_work(axis.data)), _ptr(_work(k.data)),
-                                       _ptr(_work(Ms.data)), _ptr(_work(M.data)), _ptr(out),
+    w = _works(axis, k, Ms, M)
+    check(lib().mm_uniaxial_anisotropy(_prec(), M.size(), *[_ptr(t) for t in w], _ptr(out),
                                        ctypes.byref(e), _stream()))
     if out is not H.data:
         H.data.copy_(out)
@@ -287,9 +295,9 @@ def cubic_anisotropy(axis1, axis2, k, Ms, M, H) -> float:
     """bindings/mmm/anisotropy.i:32-39."""
     e = ctypes.c_double(0.0)
     out = _work(H.data) if _mode == CUDA_32 else H.data
-    check(lib().mm_cubic_anisotropy(_prec(), M.size(), _ptr(_work(axis1.data)), _ptr(_work(axis2.data)),
-                                    _ptr(_work(k.data)), _ptr(_work(Ms.data)), _ptr(_work(M.data)),
-                                    _ptr(out), ctypes.byref(e), _stream()))
+    w = _works(axis1, axis2, k, Ms, M)
+    check(lib().mm_cubic_anisotropy(_prec(), M.size(), *[_ptr(t) for t in w], _ptr(out),
+                                    ctypes.byref(e), _stream()))
     if out is not H.data:
         H.data.copy_(out)
     return e.value
@@ -298,8 +306,8 @@ def cubic_anisotropy(axis1, axis2, k, Ms, M, H) -> float:
 def llge(f1, f2, M, H, dM) -> None:
     """bindings/mmm/llge.i:24-29: dM = f1 M x H + f2 M x (M x H)."""
     out = _work(dM.data) if _mode == CUDA_32 else dM.data
-    check(lib().mm_llge(_prec(), M.size(), _ptr(_work(f1.data)), _ptr(_work(f2.data)),
-                        _ptr(_work(M.data)), _ptr(_work(H.data)), _ptr(out), _stream()))
+    w = _works(f1, f2, M, H)
+    check(lib().mm_llge(_prec(), M.size(), *[_ptr(t) for t in w], _ptr(out), _stream()))
     if out is not dM.data:
         dM.data.copy_(out)
 
@@ -307,10 +315,9 @@ def llge(f1, f2, M, H, dM) -> None:
 def fdm_zhangli(nx, ny, nz, dx, dy, dz, do_precess, P, xi, Ms, alpha, j, M, dM) -> None:
     """bindings/mmm/zhangli.i:24-32."""
     out = _work(dM.data) if _mode == CUDA_32 else dM.data
+    w = _works(P, xi, Ms, alpha, j, M)
     check(lib().mm_fdm_zhangli(_prec(), nx, ny, nz, dx, dy, dz, int(bool(do_precess)),
-                               _ptr(_work(P.data)), _ptr(_work(xi.data)), _ptr(_work(Ms.data)),
-                               _ptr(_work(alpha.data)), _ptr(_work(j.data)), _ptr(_work(M.data)),
-                               _ptr(out), _stream()))
+                               *[_ptr(t) for t in w], _ptr(out), _stream()))
     if out is not dM.data:
         dM.data.copy_(out)
 
@@ -320,8 +327,8 @@ def scaled_abs_max(M, scale) -> float:
     if scale.isUniform():
         return M.absMax() / scale.getUniformValue()
     r = ctypes.c_double(0.0)
-    check(lib().mm_scaled_abs_max(_prec(), M.size(), _ptr(_work(M.data)), _ptr(_work(scale.data)),
-                                  ctypes.byref(r), _stream()))
+    m, sc = _works(M, scale)
+    check(lib().mm_scaled_abs_max(_prec(), M.size(), _ptr(m), _ptr(sc), ctypes.byref(r), _stream()))
     return r.value
 
 
@@ -415,8 +422,9 @@ def rk_prepare_step(step, h, tab, k0, k1, k2, k3, k4, k5, y, ytmp) -> None:
     b = (ctypes.c_double * max(step, 1))(*[tab.getB(step, j) for j in range(step)])
     arr, keep = _kptrs(ks)
     out = _work(ytmp.data) if _mode == CUDA_32 else ytmp.data
+    yw = _work(y.data)
     check(lib().mm_rk_prepare_step(_prec(), y.size(), int(step), float(h), b, arr,
-                                   _ptr(_work(y.data)), _ptr(out), _stream()))
+                                   _ptr(yw), _ptr(out), _stream()))
     if out is not ytmp.data:
         ytmp.data.copy_(out)
 

@@ -87,6 +87,14 @@ __host__ __device__ __forceinline__ V3<T> cross(V3<T> a, V3<T> b)
 	return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
 
+// Products that are never fused into an FMA with a following add/sub: keeps differences such as
+// M_j/Ms_j - M_i/Ms_i exactly zero for equal operands (the reference's CPU arithmetic does not
+// contract either).
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+template <typename T>
+__device__ __forceinline__ V3<T> scale_rn(T s, V3<T> a) { return {mul_rn(s, a.x), mul_rn(s, a.y), mul_rn(s, a.z)}; }
+
 template <typename T>
 __device__ __forceinline__ V3<T> load3(const T *p, size_t i, size_t n)
 {

@@ -221,8 +221,8 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 	if (a.terms & MM_TERM_ZHANGLI) {
 		// fdm_zhangli_cpu.cpp:100-200: u = (j.grad)M from raw M = Ms m (no Ms masking),
 		// one-sided at the borders, zero along a dimension of size 1
-		auto Mv = [&](size_t j) { return mat_of(a, j).Ms * load3(y, j, n); };
-		const V3<T> Mc = M.Ms * m;
+		auto Mv = [&](size_t j) { return scale_rn(mat_of(a, j).Ms, load3(y, j, n)); };
+		const V3<T> Mc = scale_rn(M.Ms, m);
 		auto grad = [&](int c, int dim, size_t stride, T inv1, T inv2) -> V3<T> {
 			if (dim <= 1) return v3<T>(0, 0, 0);
 			if (c == 0) return inv1 * (Mv(i + stride) - Mc);

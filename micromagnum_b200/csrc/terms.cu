@@ -40,12 +40,12 @@ __global__ void __launch_bounds__(TPB) k_exchange(int nx, int ny, int nz, double
 			continue;
 		}
 		const V3<T> Mi = load3(M, i, n);
-		const V3<T> mi = (T(1) / ms) * Mi;
+		const V3<T> mi = scale_rn(T(1) / ms, Mi);
 		V3<T> sum = v3<T>(0, 0, 0);
 		auto add = [&](size_t j, T w) {
 			const T msj = Ms[j];
 			if (msj != T(0)) {
-				const V3<T> mj = (T(1) / msj) * load3(M, j, n);
+				const V3<T> mj = scale_rn(T(1) / msj, load3(M, j, n));
 				sum = sum + w * (mj - mi);
 			}
 		};

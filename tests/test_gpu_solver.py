@@ -153,7 +153,7 @@ def test_step_semantics_rejection_and_clamp(sv, oracle_mod, ref_available):
         a, b = ours.stats, orc.stats
         assert a["t"] == pytest.approx(b["t"], rel=1e-9)
         assert a["steps"] == b["steps"] and a["rejected"] == b["rejected"]
-        assert rel_l2(ours.M.cpu().numpy(), orc.M) < 1e-11
+        assert rel_l2(ours.M.cpu().numpy(), orc.M) < 1e-9
     assert orc.stats["rejected"] > 0
 
 

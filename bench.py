@@ -108,10 +108,18 @@ class ClockSampler:
             return
         self.thread = threading.Thread(target=self._read, daemon=True)
         self.thread.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 5.0:  # nvidia-smi takes ~1 s to start
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.time(), line.strip()))
+
+    def mark(self):
+        """Start of the timed region; samples from 0.5 s before it on are kept (a short timed
+        region may fall between two 200 ms samples)."""
+        self.t_mark = time.time() - 0.5
 
     def stop(self):
         if self.proc is None:
@@ -125,7 +133,10 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        t_mark = getattr(self, "t_mark", 0.0)
+        for ts, ln in self.lines:
+            if ts < t_mark:
+                continue
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -229,6 +240,7 @@ def run_ours(args, rank, world, local_rank):
     # ---- device-resident timing ----------------------------------------------------------------
     clocks = ClockSampler(local_rank)
     clocks.start()
+    clocks.mark()
     ms, attempts, steps, launches = timed(s.step, args.steps)
     clk = clocks.stop()
     evals = 6 * attempts

@@ -302,257 +302,6 @@ __global__ void __launch_bounds__(NT) k_y_mul2d(cplx<T> *__restrict__ S, const T
 	}
 }
 
-// =================================================================================================
-// Power-of-two fast paths (fft_reg.cuh): register DFTs + one shared-memory exchange per pass.
-// =================================================================================================
-
-// y pass (3-D): TB columns x N2 threads per CTA, py = N = N1 * N2, N1 = MUL * N2.
-// Forward: reads rows y < n_in (zero above), writes all N rows; inverse: reads N rows, writes
-// rows y < n_out.  Shared memory: N * TB complex, sm[(f1 * N2 + t) * TB + b].
-template <typename T, int N1, int N2, int TB, bool INV>
-__global__ void __launch_bounds__(TB * N2) k_y_fs(cplx<T> *__restrict__ S, int n_in, int n_out, int nz, int hx,
-                                                  const cplx<T> *__restrict__ twN)
-{
-	using C = cplx<T>;
-	constexpr int N = N1 * N2;
-	constexpr int MUL = N1 / N2;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	C *sm = reinterpret_cast<C *>(smem_raw);
-	const int b = threadIdx.x, t = threadIdx.y;
-	const int kx = blockIdx.x * TB + b;
-	const bool ok = kx < hx;
-	C *base = S + (size_t)(blockIdx.z * nz + blockIdx.y) * N * hx + kx;
-	C v[N1];
-#pragma unroll
-	for (int k = 0; k < N1; ++k) {
-		const int y = t + N2 * k;
-		v[k] = (ok && y < n_in) ? base[(size_t)y * hx] : C{0, 0};
-	}
-	dft_reg<T, N1, INV>(v);
-	if constexpr (N2 == 1) {
-#pragma unroll
-		for (int f = 0; f < N1; ++f)
-			if (ok && f < n_out) base[(size_t)f * hx] = v[brev<N1>(f)];
-	} else {
-#pragma unroll
-		for (int f1 = 0; f1 < N1; ++f1) {
-			C x = v[brev<N1>(f1)];
-			if (f1 != 0 && t != 0) {
-				C w = twN[t * f1];
-				if (INV) w = conjc(w);
-				x = cmul(x, w);
-			}
-			sm[(f1 * N2 + t) * TB + b] = x;
-		}
-		__syncthreads();
-#pragma unroll
-		for (int i = 0; i < MUL; ++i) {
-			const int f1 = t + N2 * i;
-			C u[N2];
-#pragma unroll
-			for (int tt = 0; tt < N2; ++tt) u[tt] = sm[(f1 * N2 + tt) * TB + b];
-			dft_reg<T, N2, INV>(u);
-#pragma unroll
-			for (int f2 = 0; f2 < N2; ++f2) {
-				const int y = f1 + N1 * f2;
-				if (ok && y < n_out) base[(size_t)y * hx] = u[brev<N2>(f2)];
-			}
-		}
-	}
-}
-
-// z pass (3-D) with the tensor multiply: block (TB, 3), thread (b, c) owns the z column of
-// component c at x-frequency kx0 + b, y-frequency blockIdx.y.  One shared-memory exchange gives
-// each thread the three components at every kz; it forms its own row of N^ M^ in registers.
-template <typename T, int PZ, int TB>
-__global__ void __launch_bounds__(TB * 3) k_z_fs(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz, int py,
-                                                 int hx, int qy, int qz)
-{
-	using C = cplx<T>;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	C *sm = reinterpret_cast<C *>(smem_raw);  // sm[(kz * 3 + c) * TB + b]
-	const int b = threadIdx.x, c = threadIdx.y;
-	const int kx = blockIdx.x * TB + b;
-	const int ky = blockIdx.y;
-	const bool ok = kx < hx;
-	const size_t cstride = (size_t)nz * py * hx;
-	C *col = S + c * cstride + (size_t)ky * hx + kx;
-	const size_t zstride = (size_t)py * hx;
-	C v[PZ];
-#pragma unroll
-	for (int z = 0; z < PZ; ++z) v[z] = (ok && z < nz) ? col[z * zstride] : C{0, 0};
-	dft_reg<T, PZ, false>(v);
-#pragma unroll
-	for (int kz = 0; kz < PZ; ++kz) sm[(kz * 3 + c) * TB + b] = v[brev<PZ>(kz)];
-	__syncthreads();
-	const bool fy = ky > py / 2;
-	const int kyr = fy ? py - ky : ky;
-	const T sy = fy ? T(-1) : T(1);
-	const size_t cs = (size_t)qz * qy * hx;
-	// row c of the symmetric tensor: components (xx,xy,xz), (xy,yy,yz), (xz,yz,zz)
-	const int c0 = c == 0 ? 0 : (c == 1 ? 1 : 2);
-	const int c1 = c == 0 ? 1 : (c == 1 ? 3 : 4);
-	const int c2 = c == 0 ? 2 : (c == 1 ? 4 : 5);
-	const T *t0 = Nt + c0 * cs + (size_t)kyr * hx + (ok ? kx : 0);
-	const T *t1 = Nt + c1 * cs + (size_t)kyr * hx + (ok ? kx : 0);
-	const T *t2 = Nt + c2 * cs + (size_t)kyr * hx + (ok ? kx : 0);
-	const size_t kzs = (size_t)qy * hx;
-#pragma unroll
-	for (int kz = 0; kz < PZ; ++kz) {
-		constexpr int H = PZ / 2;
-		const int kzr = kz <= H ? kz : PZ - kz;
-		const T sz = kz <= H ? T(1) : T(-1);
-		// parity signs: xy ~ sy, xz ~ sz, yz ~ sy sz (diagonal components are even)
-		const T s0 = c == 0 ? T(1) : (c == 1 ? sy : sz);
-		const T s1 = c == 0 ? sy : (c == 1 ? T(1) : sy * sz);
-		const T s2 = c == 0 ? sz : (c == 1 ? sy * sz : T(1));
-		const C m0 = sm[(kz * 3 + 0) * TB + b], m1 = sm[(kz * 3 + 1) * TB + b], m2 = sm[(kz * 3 + 2) * TB + b];
-		const T n0 = s0 * t0[kzr * kzs], n1 = s1 * t1[kzr * kzs], n2 = s2 * t2[kzr * kzs];
-		v[kz] = C{n0 * m0.x + n1 * m1.x + n2 * m2.x, n0 * m0.y + n1 * m1.y + n2 * m2.y};
-	}
-	dft_reg<T, PZ, true>(v);
-#pragma unroll
-	for (int z = 0; z < PZ; ++z)
-		if (ok && z < nz) col[z * zstride] = v[brev<PZ>(z)];
-}
-
-// x pass forward: LPB complex lines per CTA, N2 threads per line; line q packs real rows 2q and
-// 2q+1 (z = a + i b).  Shared memory: N complex per line.
-template <typename T, int N1, int N2, int LPB, bool SCALE>
-__global__ void __launch_bounds__(N2 * LPB) k_x_fwd_fs(const T *__restrict__ M, const uint8_t *__restrict__ reg,
-                                                       const T *__restrict__ ms_tab, cplx<T> *__restrict__ S,
-                                                       int nx, int ny, int nz, int py, int hx,
-                                                       const cplx<T> *__restrict__ twN)
-{
-	using C = cplx<T>;
-	constexpr int N = N1 * N2;
-	constexpr int MUL = N1 / N2;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	const int t = threadIdx.x, l = threadIdx.y;
-	C *sm = reinterpret_cast<C *>(smem_raw) + (size_t)l * N;
-	const int rows = 3 * ny * nz, nyz = ny * nz;
-	const int ra = 2 * (blockIdx.x * LPB + l), rb = ra + 1;
-	const bool va = ra < rows, vb = rb < rows;
-	const T *Ma = M + (size_t)(va ? ra : 0) * nx;
-	const T *Mb = M + (size_t)(vb ? rb : 0) * nx;
-	const uint8_t *Ra = reg ? reg + (size_t)(va ? ra % nyz : 0) * nx : nullptr;
-	const uint8_t *Rb = reg ? reg + (size_t)(vb ? rb % nyz : 0) * nx : nullptr;
-	C v[N1];
-#pragma unroll
-	for (int k = 0; k < N1; ++k) {
-		const int x = t + N2 * k;
-		T a = 0, bb = 0;
-		if (x < nx) {
-			if (va) { a = Ma[x]; if (SCALE) a *= ms_tab[Ra ? Ra[x] : 0]; }
-			if (vb) { bb = Mb[x]; if (SCALE) bb *= ms_tab[Rb ? Rb[x] : 0]; }
-		}
-		v[k] = C{a, bb};
-	}
-	dft_reg<T, N1, false>(v);
-	if constexpr (N2 > 1) {
-#pragma unroll
-		for (int f1 = 0; f1 < N1; ++f1) {
-			C x = v[brev<N1>(f1)];
-			if (f1 != 0 && t != 0) x = cmul(x, twN[t * f1]);
-			sm[f1 * N2 + t] = x;
-		}
-		__syncthreads();
-		C out[MUL][N2];
-#pragma unroll
-		for (int i = 0; i < MUL; ++i) {
-			const int f1 = t + N2 * i;
-#pragma unroll
-			for (int tt = 0; tt < N2; ++tt) out[i][tt] = sm[f1 * N2 + tt];
-			dft_reg<T, N2, false>(out[i]);
-		}
-		__syncthreads();
-#pragma unroll
-		for (int i = 0; i < MUL; ++i)
-#pragma unroll
-			for (int f2 = 0; f2 < N2; ++f2) sm[t + N2 * i + N1 * f2] = out[i][brev<N2>(f2)];
-	} else {
-#pragma unroll
-		for (int f = 0; f < N1; ++f) sm[f] = v[brev<N1>(f)];
-	}
-	__syncthreads();
-	C *Sa = S + ((size_t)((va ? ra : 0) / nyz * nz + (va ? ra : 0) % nyz / ny) * py + (va ? ra : 0) % nyz % ny) * hx;
-	C *Sb = S + ((size_t)((vb ? rb : 0) / nyz * nz + (vb ? rb : 0) % nyz / ny) * py + (vb ? rb : 0) % nyz % ny) * hx;
-	const T h = T(0.5);
-	for (int k = t; k < hx; k += N2) {
-		const C zk = sm[k], zn = sm[(N - k) & (N - 1)];
-		if (va) Sa[k] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
-		if (vb) Sb[k] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
-	}
-}
-
-// x pass inverse: half spectra of rows 2q, 2q+1 -> real rows (real part / imaginary part).
-template <typename T, int N1, int N2, int LPB>
-__global__ void __launch_bounds__(N2 * LPB) k_x_inv_fs(const cplx<T> *__restrict__ S, T *__restrict__ H, int nx,
-                                                       int ny, int nz, int py, int hx,
-                                                       const cplx<T> *__restrict__ twN)
-{
-	using C = cplx<T>;
-	constexpr int N = N1 * N2;
-	constexpr int MUL = N1 / N2;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	const int t = threadIdx.x, l = threadIdx.y;
-	C *sm = reinterpret_cast<C *>(smem_raw) + (size_t)l * N;
-	const int rows = 3 * ny * nz, nyz = ny * nz;
-	const int ra = 2 * (blockIdx.x * LPB + l), rb = ra + 1;
-	const bool va = ra < rows, vb = rb < rows;
-	const int qa = va ? ra : 0, qb = vb ? rb : 0;
-	const C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * hx;
-	const C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * hx;
-	C v[N1];
-#pragma unroll
-	for (int k = 0; k < N1; ++k) {
-		const int f = t + N2 * k;
-		const bool mirror = f >= hx;
-		const int ff = mirror ? N - f : f;
-		C A = va ? Sa[ff] : C{0, 0};
-		C B = vb ? Sb[ff] : C{0, 0};
-		if (ff == 0 || 2 * ff == N) { A.y = 0; B.y = 0; }
-		if (mirror) { A.y = -A.y; B.y = -B.y; }
-		v[k] = C{A.x - B.y, A.y + B.x};
-	}
-	dft_reg<T, N1, true>(v);
-	T *Ha = H + (size_t)qa * nx, *Hb = H + (size_t)qb * nx;
-	if constexpr (N2 > 1) {
-#pragma unroll
-		for (int f1 = 0; f1 < N1; ++f1) {
-			C x = v[brev<N1>(f1)];
-			if (f1 != 0 && t != 0) x = cmul(x, conjc(twN[t * f1]));
-			sm[f1 * N2 + t] = x;
-		}
-		__syncthreads();
-#pragma unroll
-		for (int i = 0; i < MUL; ++i) {
-			const int f1 = t + N2 * i;
-			C u[N2];
-#pragma unroll
-			for (int tt = 0; tt < N2; ++tt) u[tt] = sm[f1 * N2 + tt];
-			dft_reg<T, N2, true>(u);
-#pragma unroll
-			for (int f2 = 0; f2 < N2; ++f2) {
-				const int x = f1 + N1 * f2;
-				if (x < nx) {
-					const C z = u[brev<N2>(f2)];
-					if (va) Ha[x] = z.x;
-					if (vb) Hb[x] = z.y;
-				}
-			}
-		}
-	} else {
-#pragma unroll
-		for (int x = 0; x < N1; ++x)
-			if (x < nx) {
-				const C z = v[brev<N1>(x)];
-				if (va) Ha[x] = z.x;
-				if (vb) Hb[x] = z.y;
-			}
-	}
-}
-
 // ---- set-up: generic strided complex FFT (FP64) for the tensor spectrum ------------------------
 // The array is viewed as [outer][len][inner]; line (o, i) is data[o*len*inner + k*inner + i].
 template <typename T, bool INV>
@@ -638,21 +387,183 @@ mm_status set_smem(const void *fn, size_t bytes)
 	return MM_OK;
 }
 
-// ---- fast-path geometry and dispatch ---------------------------------------------------------------
-// N = N1 * N2 with N1 = N2 or 2 N2 (N <= 32: one thread per line, N2 = 1).
-constexpr int fs_n2(int n)
+// ---- CTA-Stockham passes (cta_fft, radix 16 in registers, shared-memory passes) -----------------
+__host__ __device__ constexpr int ct_radix(int n) { return n < 16 ? n : 16; }
+__host__ __device__ constexpr int ct_radix8(int n) { return n < 8 ? n : 8; }
+__host__ __device__ constexpr int ct_tb(int n, int csize)
 {
-	return n <= 32 ? 1 : (n == 64 ? 8 : (n == 128 ? 8 : (n == 256 ? 16 : (n == 512 ? 16 : (n == 1024 ? 32 : 32)))));
-}
-constexpr int fs_tb(int n, int csize)
-{
-	// y pass: TB columns per CTA, N * TB complex in shared memory (<= 128 KB), TB * N2 <= 256 threads
 	int tb = 32;
-	while (tb > 1 && ((long)n * tb * csize > 131072 || tb * fs_n2(n) > 256)) tb >>= 1;
+	while (tb > 1 && ((long)n * tb * csize > 65536 || tb * (n / ct_radix(n)) > 512)) tb >>= 1;
 	return tb;
 }
-constexpr int fs_lpb(int n) { return 256 / fs_n2(n) > 0 ? 256 / fs_n2(n) : 1; }
-constexpr int FS_ZTB = 64;
+__host__ __device__ constexpr int ct_lpb(int n, int csize)
+{
+	int l = 256 / (n / ct_radix(n));
+	if (l < 1) l = 1;
+	while (l > 1 && (long)l * (n + 1) * csize > 65536) l >>= 1;
+	return l;
+}
+
+// y pass (3-D): TB columns per CTA; forward pads rows n_in -> N, inverse crops N -> n_out.
+template <typename T, int N, int TB, bool INV>
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
+                                                                 int hx, const cplx<T> *__restrict__ twN)
+{
+	using C = cplx<T>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *sm = reinterpret_cast<C *>(smem_raw);
+	const int tid = threadIdx.x;
+	const int line = tid & (TB - 1), j0 = tid / TB;
+	const int kx = blockIdx.x * TB + line;
+	const bool ok = kx < hx;
+	C *base = S + (size_t)(blockIdx.z * nz + blockIdx.y) * N * hx + (ok ? kx : 0);
+	auto ld = [&](int, int k) -> C { return (ok && k < n_in) ? base[(size_t)k * hx] : C{0, 0}; };
+	auto st = [&](int, int k, C v) {
+		if (ok && k < n_out) base[(size_t)k * hx] = v;
+	};
+	cta_fft<T, N, ct_radix(N), TB, INV, SmCols<N, TB>>(sm, twN, line, j0, ld, st);
+}
+
+// x pass forward: LPB complex lines per CTA (line q packs real rows 2q, 2q+1).
+template <typename T, int N, int LPB, bool SCALE>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *__restrict__ M,
+                                                                     const uint8_t *__restrict__ reg,
+                                                                     const T *__restrict__ ms_tab,
+                                                                     cplx<T> *__restrict__ S, int nx, int ny, int nz,
+                                                                     int py, int hx, const cplx<T> *__restrict__ twN)
+{
+	using C = cplx<T>;
+	constexpr int TPL = N / ct_radix(N);
+	using SI = SmRows<N, LPB>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *sm = reinterpret_cast<C *>(smem_raw);
+	const int tid = threadIdx.x;
+	const int line = tid / TPL, j0 = tid % TPL;
+	const int rows = 3 * ny * nz, nyz = ny * nz;
+	const int ra = 2 * (blockIdx.x * LPB + line), rb = ra + 1;
+	const bool va = ra < rows, vb = rb < rows;
+	const int qa = va ? ra : 0, qb = vb ? rb : 0;
+	const T *Ma = M + (size_t)qa * nx, *Mb = M + (size_t)qb * nx;
+	const uint8_t *Ra = reg ? reg + (size_t)(qa % nyz) * nx : nullptr;
+	const uint8_t *Rb = reg ? reg + (size_t)(qb % nyz) * nx : nullptr;
+	auto ld = [&](int, int x) -> C {
+		T a = 0, b = 0;
+		if (x < nx) {
+			if (va) { a = Ma[x]; if (SCALE) a *= ms_tab[Ra ? Ra[x] : 0]; }
+			if (vb) { b = Mb[x]; if (SCALE) b *= ms_tab[Rb ? Rb[x] : 0]; }
+		}
+		return C{a, b};
+	};
+	auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
+	cta_fft<T, N, ct_radix(N), LPB, false, SI>(sm, twN, line, j0, ld, st);
+	__syncthreads();
+	C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * hx;
+	C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * hx;
+	const T h = T(0.5);
+	for (int k = j0; k < hx; k += TPL) {
+		const C zk = sm[SI::at(line, k)], zn = sm[SI::at(line, (N - k) & (N - 1))];
+		if (va) Sa[k] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
+		if (vb) Sb[k] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
+	}
+}
+
+// x pass inverse: half spectra of rows 2q, 2q+1 -> real rows.
+template <typename T, int N, int LPB>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx<T> *__restrict__ S, T *__restrict__ H,
+                                                                     int nx, int ny, int nz, int py, int hx,
+                                                                     const cplx<T> *__restrict__ twN)
+{
+	using C = cplx<T>;
+	constexpr int TPL = N / ct_radix(N);
+	using SI = SmRows<N, LPB>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *sm = reinterpret_cast<C *>(smem_raw);
+	const int tid = threadIdx.x;
+	const int line = tid / TPL, j0 = tid % TPL;
+	const int rows = 3 * ny * nz, nyz = ny * nz;
+	const int ra = 2 * (blockIdx.x * LPB + line), rb = ra + 1;
+	const bool va = ra < rows, vb = rb < rows;
+	const int qa = va ? ra : 0, qb = vb ? rb : 0;
+	const C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * hx;
+	const C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * hx;
+	T *Ha = H + (size_t)qa * nx, *Hb = H + (size_t)qb * nx;
+	auto ld = [&](int, int f) -> C {
+		const bool mirror = f >= hx;
+		const int ff = mirror ? N - f : f;
+		C A = va ? Sa[ff] : C{0, 0};
+		C B = vb ? Sb[ff] : C{0, 0};
+		if (ff == 0 || 2 * ff == N) { A.y = 0; B.y = 0; }
+		if (mirror) { A.y = -A.y; B.y = -B.y; }
+		return C{A.x - B.y, A.y + B.x};
+	};
+	auto st = [&](int, int x, C v) {
+		if (x < nx) {
+			if (va) Ha[x] = v.x;
+			if (vb) Hb[x] = v.y;
+		}
+	};
+	cta_fft<T, N, ct_radix(N), LPB, true, SI>(sm, twN, line, j0, ld, st);
+}
+
+// z pass with the tensor multiply (CTA-Stockham form): lines (c, b) = c * TB + b hold the z
+// column of component c at x-frequency kx0 + b; forward transform into shared memory, multiply by
+// the real symmetric tensor (three components meet in shared memory), inverse transform to HBM.
+template <typename T, int PZ, int TB>
+__global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> *__restrict__ S,
+                                                                        const T *__restrict__ Nt, int nz, int py,
+                                                                        int hx, int qy, int qz,
+                                                                        const cplx<T> *__restrict__ twN)
+{
+	using C = cplx<T>;
+	constexpr int R = ct_radix8(PZ);
+	constexpr int LANES = 3 * TB;
+	using SI = SmCols<PZ, LANES>;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *sm = reinterpret_cast<C *>(smem_raw);
+	const int tid = threadIdx.x;
+	const int line = tid % LANES, j0 = tid / LANES;
+	const int c = line / TB, b = line % TB;
+	const int ky = blockIdx.y;
+	const size_t cstride = (size_t)nz * py * hx, zstride = (size_t)py * hx;
+	{
+		const int kx = blockIdx.x * TB + b;
+		const bool ok = kx < hx;
+		C *col = S + c * cstride + (size_t)ky * hx + (ok ? kx : 0);
+		auto ld = [&](int, int z) -> C { return (ok && z < nz) ? col[z * zstride] : C{0, 0}; };
+		auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
+		cta_fft<T, PZ, R, LANES, false, SI>(sm, twN, line, j0, ld, st);
+	}
+	__syncthreads();
+	const bool fy = ky > py / 2;
+	const int kyr = fy ? py - ky : ky;
+	const T sy = fy ? T(-1) : T(1);
+	const size_t cs = (size_t)qz * qy * hx, kzs = (size_t)qy * hx;
+	for (int idx = tid; idx < PZ * TB; idx += LANES * (PZ / R)) {
+		const int kz = idx / TB, bb = idx % TB;
+		const int kx = blockIdx.x * TB + bb;
+		if (kx >= hx) continue;
+		const bool fz = kz > PZ / 2;
+		const int kzr = fz ? PZ - kz : kz;
+		const T sz = fz ? T(-1) : T(1);
+		const T *t = Nt + (size_t)kzr * kzs + (size_t)kyr * hx + kx;
+		C &m0 = sm[SI::at(bb, kz)], &m1 = sm[SI::at(TB + bb, kz)], &m2 = sm[SI::at(2 * TB + bb, kz)];
+		tensor_apply<T, C>(t, cs, sy, sz, m0, m1, m2);
+	}
+	{
+		const int kx = blockIdx.x * TB + b;
+		const bool ok = kx < hx;
+		C *col = S + c * cstride + (size_t)ky * hx + (ok ? kx : 0);
+		auto ld = [&](int l, int k) -> C { return sm[SI::at(l, k)]; };
+		auto st = [&](int, int z, C v) {
+			if (ok && z < nz) col[z * zstride] = v;
+		};
+		__syncthreads();
+		cta_fft<T, PZ, R, LANES, true, SI, true>(sm, twN, line, j0, ld, st);
+	}
+}
+
+// ---- fast-path geometry and dispatch ---------------------------------------------------------------
+
 
 template <typename T>
 bool fs_len_ok(int n)
@@ -665,13 +576,13 @@ template <typename T, int N>
 mm_status fs_setup_len()
 {
 	using C = cplx<T>;
-	constexpr int N2 = fs_n2(N), N1 = N / N2, TB = fs_tb(N, sizeof(C)), LPB = fs_lpb(N);
-	const size_t sx = (size_t)LPB * N * sizeof(C), sy = (size_t)N * TB * sizeof(C);
-	MM_TRY(set_smem<T>((const void *)k_x_fwd_fs<T, N1, N2, LPB, false>, sx));
-	MM_TRY(set_smem<T>((const void *)k_x_fwd_fs<T, N1, N2, LPB, true>, sx));
-	MM_TRY(set_smem<T>((const void *)k_x_inv_fs<T, N1, N2, LPB>, sx));
-	MM_TRY(set_smem<T>((const void *)k_y_fs<T, N1, N2, TB, false>, sy));
-	MM_TRY(set_smem<T>((const void *)k_y_fs<T, N1, N2, TB, true>, sy));
+	constexpr int TB = ct_tb(N, sizeof(C)), LPB = ct_lpb(N, sizeof(C));
+	const size_t sx = (size_t)LPB * (N + 1) * sizeof(C), sy = (size_t)N * TB * sizeof(C);
+	MM_TRY(set_smem<T>((const void *)k_x_fwd_ct<T, N, LPB, false>, sx));
+	MM_TRY(set_smem<T>((const void *)k_x_fwd_ct<T, N, LPB, true>, sx));
+	MM_TRY(set_smem<T>((const void *)k_x_inv_ct<T, N, LPB>, sx));
+	MM_TRY(set_smem<T>((const void *)k_y_ct<T, N, TB, false>, sy));
+	MM_TRY(set_smem<T>((const void *)k_y_ct<T, N, TB, true>, sy));
 	return MM_OK;
 }
 
@@ -679,26 +590,26 @@ template <typename T, int N>
 void fs_x_fwd(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, cudaStream_t st)
 {
 	using C = cplx<T>;
-	constexpr int N2 = fs_n2(N), N1 = N / N2, LPB = fs_lpb(N);
+	constexpr int LPB = ct_lpb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
-	const dim3 grid((lines + LPB - 1) / LPB), block(N2, LPB);
-	const size_t smem = (size_t)LPB * N * sizeof(C);
+	const dim3 grid((lines + LPB - 1) / LPB), block(LPB * TPL);
+	const size_t smem = (size_t)LPB * (N + 1) * sizeof(C);
 	if (ms_tab)
-		k_x_fwd_fs<T, N1, N2, LPB, true><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
-		                                                            p->py, p->hx, (const C *)p->tw_x);
+		k_x_fwd_ct<T, N, LPB, true><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
+		                                                       p->py, p->hx, (const C *)p->tw_x);
 	else
-		k_x_fwd_fs<T, N1, N2, LPB, false><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
-		                                                             p->py, p->hx, (const C *)p->tw_x);
+		k_x_fwd_ct<T, N, LPB, false><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
+		                                                        p->py, p->hx, (const C *)p->tw_x);
 }
 
 template <typename T, int N>
 void fs_x_inv(ConvPlan *p, T *H, cudaStream_t st)
 {
 	using C = cplx<T>;
-	constexpr int N2 = fs_n2(N), N1 = N / N2, LPB = fs_lpb(N);
+	constexpr int LPB = ct_lpb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
-	const dim3 grid((lines + LPB - 1) / LPB), block(N2, LPB);
-	k_x_inv_fs<T, N1, N2, LPB><<<grid, block, (size_t)LPB * N * sizeof(C), st>>>(
+	const dim3 grid((lines + LPB - 1) / LPB), block(LPB * TPL);
+	k_x_inv_ct<T, N, LPB><<<grid, block, (size_t)LPB * (N + 1) * sizeof(C), st>>>(
 	    (const C *)p->spec, H, p->nx, p->ny, p->nz, p->py, p->hx, (const C *)p->tw_x);
 }
 
@@ -706,19 +617,21 @@ template <typename T, int N, bool INV>
 void fs_y(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
-	constexpr int N2 = fs_n2(N), N1 = N / N2, TB = fs_tb(N, sizeof(C));
-	const dim3 grid((p->hx + TB - 1) / TB, p->nz, 3), block(TB, N2);
-	k_y_fs<T, N1, N2, TB, INV><<<grid, block, (size_t)N * TB * sizeof(C), st>>>(
+	constexpr int TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
+	const dim3 grid((p->hx + TB - 1) / TB, p->nz, 3), block(TB * TPL);
+	k_y_ct<T, N, TB, INV><<<grid, block, (size_t)N * TB * sizeof(C), st>>>(
 	    (C *)p->spec, INV ? N : p->ny, INV ? p->ny : N, p->nz, p->hx, (const C *)p->tw_y);
 }
+
+constexpr int CT_ZTB = 32;
 
 template <typename T, int PZ>
 void fs_z(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
-	const dim3 grid((p->hx + FS_ZTB - 1) / FS_ZTB, p->py), block(FS_ZTB, 3);
-	k_z_fs<T, PZ, FS_ZTB><<<grid, block, (size_t)PZ * 3 * FS_ZTB * sizeof(C), st>>>(
-	    (C *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz);
+	const dim3 grid((p->hx + CT_ZTB - 1) / CT_ZTB, p->py), block(3 * CT_ZTB * (PZ / ct_radix8(PZ)));
+	k_z_ct<T, PZ, CT_ZTB><<<grid, block, (size_t)PZ * 3 * CT_ZTB * sizeof(C), st>>>(
+	    (C *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz, (const C *)p->tw_z);
 }
 
 #define MM_FS_SWITCH(n, CALL)                                                                    \
@@ -742,20 +655,21 @@ mm_status fs_setup(ConvPlan *p)
 	MM_TRY(fft_reg_init());
 	p->fast_x = fs_len_ok<T>(p->px);
 	p->fast_y = !p->is2d && fs_len_ok<T>(p->py);
-	p->fast_z = !p->is2d && p->pz >= 2 && p->pz <= 32 && (p->pz & (p->pz - 1)) == 0;
+	p->fast_z = !p->is2d && p->pz >= 2 && p->pz <= 64 && (p->pz & (p->pz - 1)) == 0;
 	mm_status r = MM_OK;
 #define MM_SETUP(N) r = fs_setup_len<T, N>()
 	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_SETUP); MM_TRY(r); }
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_SETUP); MM_TRY(r); }
 #undef MM_SETUP
 	if (p->fast_z) {
-		const size_t sz = (size_t)p->pz * 3 * FS_ZTB * sizeof(cplx<T>);
+		const size_t sz = (size_t)p->pz * 3 * CT_ZTB * sizeof(cplx<T>);
 		switch (p->pz) {
-		case 2: MM_TRY(set_smem<T>((const void *)k_z_fs<T, 2, FS_ZTB>, sz)); break;
-		case 4: MM_TRY(set_smem<T>((const void *)k_z_fs<T, 4, FS_ZTB>, sz)); break;
-		case 8: MM_TRY(set_smem<T>((const void *)k_z_fs<T, 8, FS_ZTB>, sz)); break;
-		case 16: MM_TRY(set_smem<T>((const void *)k_z_fs<T, 16, FS_ZTB>, sz)); break;
-		case 32: MM_TRY(set_smem<T>((const void *)k_z_fs<T, 32, FS_ZTB>, sz)); break;
+		case 2: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 2, CT_ZTB>, sz)); break;
+		case 4: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 4, CT_ZTB>, sz)); break;
+		case 8: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 8, CT_ZTB>, sz)); break;
+		case 16: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 16, CT_ZTB>, sz)); break;
+		case 32: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 32, CT_ZTB>, sz)); break;
+		case 64: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 64, CT_ZTB>, sz)); break;
 		}
 	}
 	return MM_OK;
@@ -915,6 +829,7 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 			case 8: fs_z<T, 8>(p, st); break;
 			case 16: fs_z<T, 16>(p, st); break;
 			case 32: fs_z<T, 32>(p, st); break;
+			case 64: fs_z<T, 64>(p, st); break;
 			}
 		} else
 			k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz,

@@ -67,3 +67,87 @@ __device__ __forceinline__ void dft_reg(cplx<T> (&v)[N])
 }
 
 } // namespace mm
+
+namespace mm {
+
+// ---- CTA-wide Stockham FFT with compile-time length and radix -----------------------------------
+// LANES independent lines of length N live in shared memory; each of the N/R threads of a line
+// performs R/Rp radix-Rp butterflies per pass (Rp = R except possibly a smaller last pass).  Pass 0
+// reads its inputs through `ld(line, k)` (global memory, with zero padding), the last pass hands
+// its outputs to `st(line, k, value)`; intermediate passes go through shared memory at
+// `SmIdx::at(line, k)`.  All strides are compile-time powers of two.
+__host__ __device__ constexpr int ilog2c(int n) { return n <= 1 ? 0 : 1 + ilog2c(n / 2); }
+__host__ __device__ constexpr int fft_npasses(int N, int R) { return (ilog2c(N) + ilog2c(R) - 1) / ilog2c(R); }
+__host__ __device__ constexpr int fft_radix(int N, int R, int p)
+{
+	return ilog2c(N) - p * ilog2c(R) >= ilog2c(R) ? R : (1 << (ilog2c(N) - p * ilog2c(R)));
+}
+
+template <int N, int LANES>
+struct SmCols {  // element (line, k) at k * LANES + line: lines are adjacent columns
+	__device__ __forceinline__ static int at(int line, int k) { return k * LANES + line; }
+};
+template <int N, int LANES>
+struct SmRows {  // element (line, k) at line * (N + 1) + k: one padded row per line
+	__device__ __forceinline__ static int at(int line, int k) { return line * (N + 1) + k; }
+};
+
+template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, class LD, class ST>
+__device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0,
+                                             LD &ld, ST &st)
+{
+	using C = cplx<T>;
+	constexpr int P = fft_npasses(N, R);
+	constexpr int Rp = fft_radix(N, R, p);
+	constexpr int Ns = 1 << (p * ilog2c(R));  // product of the radices of earlier passes
+	constexpr int TPL = N / R;
+	constexpr int BPT = R / Rp;
+	constexpr int M = N / Rp;                  // butterflies per line, input stride
+	C v[BPT][Rp];
+	if constexpr (p > 0) __syncthreads();
+#pragma unroll
+	for (int u = 0; u < BPT; ++u) {
+		const int j = j0 + u * TPL;
+#pragma unroll
+		for (int q = 0; q < Rp; ++q) {
+			if constexpr (p == 0) v[u][q] = ld(line, j + q * M);
+			else v[u][q] = sm[SmIdx::at(line, j + q * M)];
+		}
+	}
+	if constexpr (p > 0 || LD_SM) __syncthreads();  // all inputs read before any output lands
+#pragma unroll
+	for (int u = 0; u < BPT; ++u) {
+		const int j = j0 + u * TPL;
+		const int jm = j & (Ns - 1);
+		if constexpr (Ns > 1) {
+			if (jm != 0) {
+#pragma unroll
+				for (int q = 1; q < Rp; ++q) {
+					C w = twN[q * jm * (N / (Ns * Rp))];
+					if (INV) w = conjc(w);
+					v[u][q] = cmul(v[u][q], w);
+				}
+			}
+		}
+		dft_reg<T, Rp, INV>(v[u]);
+		const int base = (j / Ns) * Ns * Rp + jm;
+#pragma unroll
+		for (int k = 0; k < Rp; ++k) {
+			const C val = v[u][brev<Rp>(k)];
+			if constexpr (p == P - 1) st(line, base + k * Ns, val);
+			else sm[SmIdx::at(line, base + k * Ns)] = val;
+		}
+	}
+	if constexpr (p + 1 < P) cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, p + 1>(sm, twN, line, j0, ld, st);
+}
+
+// LD_SM: the loader reads the same shared memory the passes write (adds a barrier after pass 0's
+// reads).
+template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM = false, class LD, class ST>
+__device__ __forceinline__ void cta_fft(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0, LD &ld,
+                                        ST &st)
+{
+	cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, 0>(sm, twN, line, j0, ld, st);
+}
+
+} // namespace mm

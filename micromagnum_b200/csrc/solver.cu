@@ -502,6 +502,14 @@ struct mm_solver {
 	void *kh[MAXS] = {};
 	CellArgs<double> args64{};
 	CellArgs<float> args32{};
+	// captured attempts (index: first stage evaluated or reused) and their kernel counts
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+	uint64_t gkernels[2] = {0, 0};
+	int glast[2] = {0, 0};
+	// graphs are captured and replayed on a private stream (capture is not allowed on the legacy
+	// default stream), ordered after / before the caller's stream with events
+	cudaStream_t gs = nullptr;
+	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 };
 
 namespace mm {
@@ -756,14 +764,73 @@ mm_status put_time(mm_solver *s, double t, double h, cudaStream_t st)
 	return MM_OK;
 }
 
+// One attempt + controller as a CUDA graph: the H2D copy of (t, h) from the pinned host state,
+// the demag passes and fused stages, and the controller, replayed with a single launch.  Kernel
+// parameters never change between attempts (step size and time are read from device memory, the
+// first-same-as-last exchange is a device-side pointer swap), so one graph per variant serves the
+// whole run.
+template <typename T>
+mm_status attempt_graph(mm_solver *s, bool eval_k0, cudaStream_t st)
+{
+	const int v = eval_k0 ? 1 : 0;
+	if (!s->gs) {
+		MM_CUDA(cudaStreamCreateWithFlags(&s->gs, cudaStreamNonBlocking));
+		MM_CUDA(cudaEventCreateWithFlags(&s->ev_in, cudaEventDisableTiming));
+		MM_CUDA(cudaEventCreateWithFlags(&s->ev_out, cudaEventDisableTiming));
+	}
+	cudaStream_t user = st;
+	st = s->gs;
+	MM_CUDA(cudaEventRecord(s->ev_in, user));
+	MM_CUDA(cudaStreamWaitEvent(st, s->ev_in, 0));
+	if (!s->gexec[v]) {
+		const uint64_t before = launch_counter().load();
+		MM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+		mm_status r = cuda_status(cudaMemcpyAsync(s->dst, s->hst, 2 * sizeof(double), cudaMemcpyHostToDevice, st),
+		                          "cudaMemcpyAsync");
+		if (r == MM_OK) r = attempt<T>(s, eval_k0, st);
+		if (r == MM_OK) {
+			k_controller<T><<<1, 1, 0, st>>>(s->dst, (KTab<T> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
+			                                 s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+			r = after_launch("k_controller");
+		}
+		cudaGraph_t g = nullptr;
+		const cudaError_t e = cudaStreamEndCapture(st, &g);
+		if (r != MM_OK) {
+			if (g) cudaGraphDestroy(g);
+			return r;
+		}
+		MM_CUDA(e);
+		const cudaError_t ei = cudaGraphInstantiate(&s->gexec[v], g, 0);
+		cudaGraphDestroy(g);
+		MM_CUDA(ei);
+		s->gkernels[v] = launch_counter().load() - before;
+		launch_counter().fetch_sub(s->gkernels[v]);  // counted when the graph runs
+		s->glast[v] = s->last_stage_buf;
+	}
+	MM_CUDA(cudaGraphLaunch(s->gexec[v], st));
+	launch_counter().fetch_add(s->gkernels[v]);
+	s->last_stage_buf = s->glast[v];
+	MM_CUDA(cudaEventRecord(s->ev_out, st));
+	MM_CUDA(cudaStreamWaitEvent(user, s->ev_out, 0));
+	return MM_OK;
+}
+
 // One attempt + controller; returns the decision in s->hst.
 template <typename T>
 mm_status attempt_and_control(mm_solver *s, double h, cudaStream_t st)
 {
-	MM_TRY(put_time(s, s->t, h, st));
 	const bool eval_k0 = !(s->tab.fsal && s->k0_valid);
-	MM_TRY(attempt<T>(s, eval_k0, st));
-	MM_TRY(controller<T>(s, st));
+	if (profiling_on()) {
+		// per-kernel event timing needs direct launches
+		MM_TRY(put_time(s, s->t, h, st));
+		MM_TRY(attempt<T>(s, eval_k0, st));
+		MM_TRY(controller<T>(s, st));
+	} else {
+		s->hst->t = s->t;
+		s->hst->h = h;
+		MM_TRY(attempt_graph<T>(s, eval_k0, st));
+		MM_CUDA(cudaStreamSynchronize(st));
+	}
 	s->attempts++;
 	if (s->tab.fsal) s->k0_valid = true;
 	return MM_OK;
@@ -794,11 +861,9 @@ mm_status evolve(mm_solver *s, double t_max, cudaStream_t st)
 	if (s->t + h_try > t_max) {
 		// runge_kutta.py:75-78: redo the step with the clamped size, accepted without a check
 		h_try = t_max - s->t;
-		MM_TRY(put_time(s, s->t, h_try, st));
-		MM_TRY(attempt<T>(s, !(s->tab.fsal && s->k0_valid), st));
-		MM_TRY(controller<T>(s, st));  // keeps the reductions reset and the FSAL swap in step
-		s->attempts++;
-		if (s->tab.fsal) s->k0_valid = true;
+		// the controller's decision is ignored; it keeps the reductions reset and the
+		// first-same-as-last swap in step
+		MM_TRY(attempt_and_control<T>(s, h_try, st));
 	}
 	MM_TRY(accept_state<T>(s, st));
 	s->t += h_try;
@@ -826,6 +891,11 @@ mm_status average(mm_solver *s, double *out3, cudaStream_t st)
 void free_solver(mm_solver *s)
 {
 	if (!s) return;
+	for (int v = 0; v < 2; ++v)
+		if (s->gexec[v]) cudaGraphExecDestroy(s->gexec[v]);
+	if (s->gs) cudaStreamDestroy(s->gs);
+	if (s->ev_in) cudaEventDestroy(s->ev_in);
+	if (s->ev_out) cudaEventDestroy(s->ev_out);
 	delete s->conv;
 	cudaFree(s->mat);
 	cudaFree(s->ms_tab);

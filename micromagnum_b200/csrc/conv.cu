@@ -400,7 +400,7 @@ __host__ __device__ constexpr int ct_lpb(int n, int csize)
 {
 	int l = 256 / (n / ct_radix(n));
 	if (l < 1) l = 1;
-	while (l > 1 && (long)l * (n + 1) * csize > 65536) l >>= 1;
+	while (l > 1 && (long)(l * n + (l * n >> 5) + 1) * csize > 65536) l >>= 1;
 	return l;
 }
 
@@ -577,7 +577,7 @@ mm_status fs_setup_len()
 {
 	using C = cplx<T>;
 	constexpr int TB = ct_tb(N, sizeof(C)), LPB = ct_lpb(N, sizeof(C));
-	const size_t sx = (size_t)LPB * (N + 1) * sizeof(C), sy = (size_t)N * TB * sizeof(C);
+	const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
 	MM_TRY(set_smem<T>((const void *)k_x_fwd_ct<T, N, LPB, false>, sx));
 	MM_TRY(set_smem<T>((const void *)k_x_fwd_ct<T, N, LPB, true>, sx));
 	MM_TRY(set_smem<T>((const void *)k_x_inv_ct<T, N, LPB>, sx));
@@ -593,7 +593,7 @@ void fs_x_fwd(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, cuda
 	constexpr int LPB = ct_lpb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
 	const dim3 grid((lines + LPB - 1) / LPB), block(LPB * TPL);
-	const size_t smem = (size_t)LPB * (N + 1) * sizeof(C);
+	const size_t smem = (size_t)SmRows<N, LPB>::SIZE * sizeof(C);
 	if (ms_tab)
 		k_x_fwd_ct<T, N, LPB, true><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
 		                                                       p->py, p->hx, (const C *)p->tw_x);
@@ -609,7 +609,7 @@ void fs_x_inv(ConvPlan *p, T *H, cudaStream_t st)
 	constexpr int LPB = ct_lpb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
 	const dim3 grid((lines + LPB - 1) / LPB), block(LPB * TPL);
-	k_x_inv_ct<T, N, LPB><<<grid, block, (size_t)LPB * (N + 1) * sizeof(C), st>>>(
+	k_x_inv_ct<T, N, LPB><<<grid, block, (size_t)SmRows<N, LPB>::SIZE * sizeof(C), st>>>(
 	    (const C *)p->spec, H, p->nx, p->ny, p->nz, p->py, p->hx, (const C *)p->tw_x);
 }
 
@@ -619,7 +619,7 @@ void fs_y(ConvPlan *p, cudaStream_t st)
 	using C = cplx<T>;
 	constexpr int TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const dim3 grid((p->hx + TB - 1) / TB, p->nz, 3), block(TB * TPL);
-	k_y_ct<T, N, TB, INV><<<grid, block, (size_t)N * TB * sizeof(C), st>>>(
+	k_y_ct<T, N, TB, INV><<<grid, block, (size_t)SmCols<N, TB>::SIZE * sizeof(C), st>>>(
 	    (C *)p->spec, INV ? N : p->ny, INV ? p->ny : N, p->nz, p->hx, (const C *)p->tw_y);
 }
 
@@ -630,7 +630,7 @@ void fs_z(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
 	const dim3 grid((p->hx + CT_ZTB - 1) / CT_ZTB, p->py), block(3 * CT_ZTB * (PZ / ct_radix8(PZ)));
-	k_z_ct<T, PZ, CT_ZTB><<<grid, block, (size_t)PZ * 3 * CT_ZTB * sizeof(C), st>>>(
+	k_z_ct<T, PZ, CT_ZTB><<<grid, block, (size_t)SmCols<PZ, 3 * CT_ZTB>::SIZE * sizeof(C), st>>>(
 	    (C *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz, (const C *)p->tw_z);
 }
 
@@ -662,7 +662,7 @@ mm_status fs_setup(ConvPlan *p)
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_SETUP); MM_TRY(r); }
 #undef MM_SETUP
 	if (p->fast_z) {
-		const size_t sz = (size_t)p->pz * 3 * CT_ZTB * sizeof(cplx<T>);
+		const size_t sz = (size_t)(p->pz * 3 * CT_ZTB + (p->pz * 3 * CT_ZTB >> 5) + 1) * sizeof(cplx<T>);
 		switch (p->pz) {
 		case 2: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 2, CT_ZTB>, sz)); break;
 		case 4: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 4, CT_ZTB>, sz)); break;

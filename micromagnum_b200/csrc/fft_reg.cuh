@@ -83,13 +83,18 @@ __host__ __device__ constexpr int fft_radix(int N, int R, int p)
 	return ilog2c(N) - p * ilog2c(R) >= ilog2c(R) ? R : (1 << (ilog2c(N) - p * ilog2c(R)));
 }
 
+// Shared-memory layouts.  One padding slot per 32 elements skews the Stockham pass-0 writes
+// (stride R) and the column tiles across the banks.
+__host__ __device__ constexpr int sm_pad(int raw) { return raw + (raw >> 5); }
 template <int N, int LANES>
 struct SmCols {  // element (line, k) at k * LANES + line: lines are adjacent columns
-	__device__ __forceinline__ static int at(int line, int k) { return k * LANES + line; }
+	static constexpr int SIZE = N * LANES + (N * LANES >> 5) + 1;
+	__device__ __forceinline__ static int at(int line, int k) { return sm_pad(k * LANES + line); }
 };
 template <int N, int LANES>
-struct SmRows {  // element (line, k) at line * (N + 1) + k: one padded row per line
-	__device__ __forceinline__ static int at(int line, int k) { return line * (N + 1) + k; }
+struct SmRows {  // element (line, k) at line * N + k
+	static constexpr int SIZE = N * LANES + (N * LANES >> 5) + 1;
+	__device__ __forceinline__ static int at(int line, int k) { return sm_pad(line * N + k); }
 };
 
 template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, class LD, class ST>

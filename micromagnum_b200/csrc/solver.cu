@@ -149,6 +149,7 @@ struct CellArgs {
 	int terms;
 	const uint8_t *reg;            // nullptr: every cell is region 0
 	const DevMat<T> *mat;
+	int nmat;
 	double Hext[3], Hpulse[3], rise;
 };
 
@@ -159,11 +160,13 @@ __device__ __forceinline__ const DevMat<T> &mat_of(const CellArgs<T> &a, size_t 
 }
 
 // Effective field (without the demag term) and dm/dt of one cell of the unit-m field y.
-// Hd: demag field of the cell (added when the term is on).  Returns false for empty cells.
+// Hd: demag field of the cell (added when the term is on); msr: Ms per region (shared memory).
+// The six neighbours are loaded once and serve both the exchange stencil and the Zhang-Li
+// gradient.  Returns false for empty cells.
 template <typename T>
-__device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restrict__ y, size_t n,
-                                         int x, int yy, int z, size_t i, V3<T> Hd, double t,
-                                         V3<T> &Heff, V3<T> &dm)
+__device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restrict__ msr,
+                                         const T *__restrict__ y, size_t n, int x, int yy, int z, size_t i,
+                                         V3<T> Hd, double t, V3<T> &Heff, V3<T> &dm)
 {
 	const DevMat<T> &M = mat_of(a, i);
 	double f = 1.0;
@@ -172,7 +175,8 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 	                     ? v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
 	                             (T)(a.Hext[2] + a.Hpulse[2] * f))
 	                     : v3<T>(0, 0, 0);
-	if (M.Ms == T(0)) {
+	const T ms = M.Ms;
+	if (ms == T(0)) {
 		// empty cell: no magnetisation and no torque, but the stray and applied fields exist
 		// there (H_tot is the sum of the terms, each zero except these two)
 		Heff = ((a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0)) + Hz;
@@ -181,22 +185,29 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 	}
 	const V3<T> m = load3(y, i, n);
 	const size_t nxy = (size_t)a.nx * a.ny;
+	const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
+	const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
+	V3<T> nb[6];
+	T nms[6];
+#pragma unroll
+	for (int q = 0; q < 6; ++q) {
+		if (has[q]) {
+			nb[q] = load3(y, off[q], n);
+			nms[q] = a.reg ? msr[a.reg[off[q]]] : ms;
+		} else {
+			nb[q] = v3<T>(0, 0, 0);
+			nms[q] = T(0);
+		}
+	}
 	V3<T> H = (a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0);
-	// neighbour indices (valid flags)
-	const bool hl = x > 0, hr = x < a.nx - 1, hd = yy > 0, hu = yy < a.ny - 1, hb = z > 0, hf = z < a.nz - 1;
 	if (a.terms & MM_TERM_EXCHANGE) {
 		// exchange_cpu.cpp:60-139: H = 2A/(mu0 Ms) sum_nb w (m_nb - m), empty neighbours skipped
-		V3<T> s = v3<T>(0, 0, 0);
-		auto nb = [&](bool ok, size_t j, T w) {
-			if (ok && mat_of(a, j).Ms != T(0)) s = s + w * (load3(y, j, n) - m);
-		};
-		nb(hl, i - 1, a.wx);
-		nb(hr, i + 1, a.wx);
-		nb(hd, i - a.nx, a.wy);
-		nb(hu, i + a.nx, a.wy);
-		nb(hb, i - nxy, a.wz);
-		nb(hf, i + nxy, a.wz);
-		H = H + M.cex * s;
+		const T w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
+		V3<T> sum = v3<T>(0, 0, 0);
+#pragma unroll
+		for (int q = 0; q < 6; ++q)
+			if (nms[q] != T(0)) sum = sum + w[q] * (nb[q] - m);
+		H = H + M.cex * sum;
 	}
 	if (a.terms & MM_TERM_UNIAXIAL) {
 		// anisotropy_cpu.cpp:29-73 (k == 0 gives ku == 0)
@@ -221,25 +232,32 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 	if (a.terms & MM_TERM_ZHANGLI) {
 		// fdm_zhangli_cpu.cpp:100-200: u = (j.grad)M from raw M = Ms m (no Ms masking),
 		// one-sided at the borders, zero along a dimension of size 1
-		auto Mv = [&](size_t j) { return scale_rn(mat_of(a, j).Ms, load3(y, j, n)); };
-		const V3<T> Mc = scale_rn(M.Ms, m);
-		auto grad = [&](int c, int dim, size_t stride, T inv1, T inv2) -> V3<T> {
+		const V3<T> Mc = scale_rn(ms, m);
+		auto grad = [&](int c, int dim, int lo, T inv1, T inv2) -> V3<T> {
 			if (dim <= 1) return v3<T>(0, 0, 0);
-			if (c == 0) return inv1 * (Mv(i + stride) - Mc);
-			if (c == dim - 1) return inv1 * (Mc - Mv(i - stride));
-			return inv2 * (Mv(i + stride) - Mv(i - stride));
+			const V3<T> Ml = scale_rn(nms[lo], nb[lo]), Mr = scale_rn(nms[lo + 1], nb[lo + 1]);
+			if (c == 0) return inv1 * (Mr - Mc);
+			if (c == dim - 1) return inv1 * (Mc - Ml);
+			return inv2 * (Mr - Ml);
 		};
-		const V3<T> gx = grad(x, a.nx, 1, a.idx1, a.idx2);
-		const V3<T> gy = grad(yy, a.ny, a.nx, a.idy1, a.idy2);
-		const V3<T> gz = grad(z, a.nz, nxy, a.idz1, a.idz2);
-		const T inv = T(1) / M.Ms;
-		const V3<T> u = inv * v3<T>(M.j[0] * gx.x + M.j[1] * gy.x + M.j[2] * gz.x,
-		                            M.j[0] * gx.y + M.j[1] * gy.y + M.j[2] * gz.y,
-		                            M.j[0] * gx.z + M.j[1] * gy.z + M.j[2] * gz.z);
+		V3<T> u = v3<T>(0, 0, 0);
+		if (M.j[0] != T(0)) u = u + M.j[0] * grad(x, a.nx, 0, a.idx1, a.idx2);
+		if (M.j[1] != T(0)) u = u + M.j[1] * grad(yy, a.ny, 2, a.idy1, a.idy2);
+		if (M.j[2] != T(0)) u = u + M.j[2] * grad(z, a.nz, 4, a.idz1, a.idz2);
+		u = (T(1) / ms) * u;
 		const V3<T> mxu = cross(m, u);
 		dm = dm + M.zl1 * cross(m, mxu) + M.zl2 * mxu;
 	}
 	return true;
+}
+
+// Ms per region into shared memory (all threads of the block call this).
+template <typename T>
+__device__ __forceinline__ void load_ms_table(const CellArgs<T> &a, T *msr)
+{
+	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+	for (int r = tid; r < a.nmat; r += blockDim.x * blockDim.y) msr[r] = a.mat[r].Ms;
+	__syncthreads();
 }
 
 // Per-stage coefficients (by value).
@@ -256,7 +274,11 @@ struct StageCoef {
 
 // One fused stage: k_i = f(y_in) (demag field from Hd), then the next stage state
 // y_{i+1} = y_n + h sum_{l<=i} b_{i+1,l} k_l, or on the last stage the error maximum and y_{n+1}.
-// COMP: compensated float state (y_n = yhi + ylo).
+// COMP: compensated float state (y_n = yhi + ylo).  Each thread handles CPT cells 32 apart in x
+// (every warp access stays a contiguous 128-byte run) and issues all their loads before any
+// store, so twice the bytes are in flight per thread.
+constexpr int STAGE_CPT = 2;
+
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
                                                const T *__restrict__ y_in, const T *__restrict__ Hd,
@@ -265,20 +287,33 @@ __global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
                                                T *__restrict__ y_out_lo, const DevState *__restrict__ st,
                                                double *red_err, double *red_k0)
 {
-	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	__shared__ T msr[256];
+	load_ms_table(a, msr);
 	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
 	const int z = blockIdx.z;
-	const bool inside = x < a.nx && yy < a.ny;
 	const size_t n = (size_t)a.nx * a.ny * a.nz;
-	const size_t i = ((size_t)z * a.ny + (inside ? yy : 0)) * a.nx + (inside ? x : 0);
 	const double h = st->h;
+	const double t = st->t + sc.a_i * h;
+	T *const *K = ktab->k;
+	V3<T> ki[STAGE_CPT];
+	size_t idx[STAGE_CPT];
+	bool in[STAGE_CPT];
+#pragma unroll
+	for (int u = 0; u < STAGE_CPT; ++u) {
+		const int x = blockIdx.x * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
+		in[u] = x < a.nx && yy < a.ny;
+		idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
+		if (in[u]) {
+			V3<T> Heff;
+			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
+			cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
+		}
+	}
 	T e2 = T(0), k02 = T(0);
-	if (inside) {
-		V3<T> Heff, ki;
-		const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, i, n) : v3<T>(0, 0, 0);
-		cell_rhs<T>(a, y_in, n, x, yy, z, i, hd, st->t + sc.a_i * h, Heff, ki);
-		T *const *K = ktab->k;
-		store3(K[sc.stage], i, n, ki);
+#pragma unroll
+	for (int u = 0; u < STAGE_CPT; ++u) {
+		if (!in[u]) continue;
+		const size_t i = idx[u];
 		if (!sc.last) {
 			if (sc.write_next) {
 				V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
@@ -286,13 +321,13 @@ __global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
 					const T f = (T)(h * sc.bn[l]);
 					if (f != T(0)) acc = acc + f * load3(K[l], i, n);
 				}
-				acc = acc + (T)(h * sc.bn[sc.stage]) * ki;
+				acc = acc + (T)(h * sc.bn[sc.stage]) * ki[u];
 				if (COMP) acc = load3(yhi, i, n) + acc;
 				store3(y_out, i, n, acc);
 			}
 			if (sc.reduce_k0) {
-				const V3<T> k0 = sc.stage == 0 ? ki : load3(K[0], i, n);
-				k02 = dot(k0, k0);
+				const V3<T> k0 = sc.stage == 0 ? ki[u] : load3(K[0], i, n);
+				k02 = max(k02, dot(k0, k0));
 			}
 		} else {
 			V3<T> err = v3<T>(0, 0, 0);
@@ -301,11 +336,11 @@ __global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
 				const T fe = (T)(h * sc.ec[l]);
 				const T fc = (T)(h * sc.bn[l]);
 				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
-				const V3<T> kl = l == sc.stage ? ki : load3(K[l], i, n);
+				const V3<T> kl = l == sc.stage ? ki[u] : load3(K[l], i, n);
 				err = err + fe * kl;
 				if (sc.write_new) acc = acc + fc * kl;
 			}
-			e2 = dot(err, err);
+			e2 = nan_max(e2, dot(err, err));
 			if (sc.write_new) {
 				if (COMP) {
 					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
@@ -321,6 +356,7 @@ __global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
 				}
 			}
 		}
+		store3(K[sc.stage], i, n, ki[u]);
 	}
 	if (sc.last) block_max_to(red_err, e2);
 	if (sc.reduce_k0) block_max_to(red_k0, k02);
@@ -401,6 +437,8 @@ __global__ void __launch_bounds__(256) k_eval(CellArgs<T> a, const T *__restrict
                                               double *__restrict__ dMdt_out,
                                               double *__restrict__ Hd_out)
 {
+	__shared__ T msr[256];
+	load_ms_table(a, msr);
 	const int x = blockIdx.x * blockDim.x + threadIdx.x;
 	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
 	const int z = blockIdx.z;
@@ -409,7 +447,7 @@ __global__ void __launch_bounds__(256) k_eval(CellArgs<T> a, const T *__restrict
 	const size_t i = ((size_t)z * a.ny + yy) * a.nx + x;
 	V3<T> Heff, dm;
 	const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, i, n) : v3<T>(0, 0, 0);
-	cell_rhs<T>(a, m, n, x, yy, z, i, hd, t, Heff, dm);
+	cell_rhs<T>(a, msr, m, n, x, yy, z, i, hd, t, Heff, dm);
 	const double ms = (double)mat_of(a, i).Ms;
 	if (Heff_out) { Heff_out[i] = Heff.x; Heff_out[i + n] = Heff.y; Heff_out[i + 2 * n] = Heff.z; }
 	if (dMdt_out) { dMdt_out[i] = ms * dm.x; dMdt_out[i + n] = ms * dm.y; dMdt_out[i + 2 * n] = ms * dm.z; }
@@ -491,6 +529,7 @@ struct mm_solver {
 	double *avg = nullptr;                     // device scratch for <M>
 	double *avg_h = nullptr;                   // pinned
 	int last_stage_buf = 0;                    // ys[] index holding y_{n+1}
+	int nmat = 1;
 	// host-side solver state (RungeKutta.evolve semantics, runge_kutta.py:47-87)
 	double t = 0, h = 0, h_next = 0;
 	bool have_next = false;
@@ -533,6 +572,7 @@ void fill_args(mm_solver *s, CellArgs<T> &a)
 	a.terms = c.terms;
 	a.reg = s->reg;
 	a.mat = (const DevMat<T> *)s->mat;
+	a.nmat = s->nmat;
 	for (int q = 0; q < 3; ++q) { a.Hext[q] = c.H_ext[q]; a.Hpulse[q] = c.H_pulse[q]; }
 	a.rise = c.pulse_rise;
 }
@@ -623,6 +663,10 @@ template <>
 const CellArgs<float> &args_of<float>(mm_solver *s) { return s->args32; }
 
 dim3 cell_grid(const mm_solver_config &c) { return dim3((c.nx + 31) / 32, (c.ny + 7) / 8, c.nz); }
+dim3 stage_grid(const mm_solver_config &c)
+{
+	return dim3((c.nx + 32 * STAGE_CPT - 1) / (32 * STAGE_CPT), (c.ny + 7) / 8, c.nz);
+}
 
 // Demag field of the state y (unit, T) into s->hd.
 template <typename T>
@@ -680,7 +724,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 	constexpr bool COMP = sizeof(T) == 4;
 	const Tableau &tb = s->tab;
 	const CellArgs<T> &a = args_of<T>(s);
-	const dim3 grid = cell_grid(s->cfg), block(32, 8, 1);
+	const dim3 grid = stage_grid(s->cfg), block(32, 8, 1);
 	DevState *ds = s->dst;
 	double *red_err = &ds->max_err2, *red_k0 = &ds->max_k02;
 	const T *yhi = (const T *)s->m, *ylo = (const T *)s->m_lo;
@@ -919,6 +963,7 @@ template <typename T>
 mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uint8_t *regions,
                       const double *tensor, cudaStream_t st)
 {
+	s->nmat = nmat;
 	MM_TRY(build_materials<T>(s, nmat, mats));
 	if (regions) {
 		for (size_t i = 0; i < s->n; ++i)

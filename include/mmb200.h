@@ -115,6 +115,21 @@ MM_API mm_status mm_fdm_zhangli(int prec, int nx, int ny, int nz, double dx, dou
 MM_API mm_status mm_scaled_abs_max(int prec, size_t n, const void *M, const void *scale,
                                    double *result_host, void *stream);
 
+/* The same result as mm_scaled_abs_max, computed without allocating any memory.  No counterpart
+ * in the reference: it exists for callers that must not allocate once their set-up is done, such
+ * as a process whose free device memory is already reserved by a pool (a late cudaMalloc would
+ * fail there) or a step loop that must not meet the synchronisation a cudaMalloc/cudaMallocHost
+ * can imply; mm_scaled_abs_max allocates a device accumulator and a pinned host word on its
+ * first call on each device.  Scratch is a fixed 512 KiB array in the library's static device
+ * memory: at most 65536 partial maxima of 4096 cells, so n is limited to 268,435,456 cells and
+ * larger n returns MM_ERR_INVALID_ARGUMENT.  Nothing in the scratch has to start at zero.  The
+ * first call on each device (with that device current) looks up the array's address; make it
+ * during set-up, before any stream capture.  Every call on a device uses the same array, so
+ * calls that overlap on the device (other streams, other host threads) race: serialise them.
+ * Synchronises `stream`. */
+MM_API mm_status mm_scaled_abs_max_noalloc(int prec, size_t n, const void *M, const void *scale,
+                                           double *result_host, void *stream);
+
 /* M_i <- Ms_i M_i / |M_i| (0 where |M_i| == 0).  Replaces VectorMatrix::normalize(Matrix)
  * (matrix/matrix/vector/VectorMatrix.cpp:218-230) as called by the solver after every accepted
  * step (magnum/micromagnetics/micro_magnetics.py:49-50). */

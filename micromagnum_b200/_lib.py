@@ -78,6 +78,7 @@ _PROTOS = [
     ("mm_llge", _I, [_I, _SZ, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("mm_fdm_zhangli", _I, [_I, _I, _I, _I, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("mm_scaled_abs_max", _I, [_I, _SZ, _VP, _VP, _DP, _VP]),
+    ("mm_scaled_abs_max_noalloc", _I, [_I, _SZ, _VP, _VP, _DP, _VP]),
     ("mm_normalize", _I, [_I, _SZ, _VP, _VP, _VP]),
     ("mm_rk_prepare_step", _I, [_I, _SZ, _I, _D, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
     ("mm_rk_combine_result", _I, [_I, _SZ, _I, _D, _DP, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),

@@ -7,6 +7,8 @@
 // warp reads 32 consecutive elements of each SoA array.
 #include "mm_common.cuh"
 
+#include <mutex>
+
 namespace mm {
 namespace {
 
@@ -504,6 +506,138 @@ MM_API mm_status mm_rk_combine_result(int prec, size_t n, int nk, double h, cons
 		k_rk_combine<float><<<grid_for(n3), TPB, 0, st>>>(n3, nk, h, kp, (float *)y, (float *)y_error);
 	}
 	return after_launch("k_rk_combine");
+}
+
+} // extern "C"
+
+// ---- scaled_abs_max without allocation ------------------------------------------------------------
+// mm_scaled_abs_max_noalloc returns what mm_scaled_abs_max returns, for callers that must not
+// allocate memory once their set-up is done.  mm_scaled_abs_max creates a device accumulator
+// (cudaMalloc) and a pinned host word (cudaMallocHost) on its first call on each device; a caller
+// whose device memory is already handed out to a pool (so that a late cudaMalloc fails), or whose
+// step loop must not meet the device-wide synchronisation a cudaMalloc/cudaMallocHost can imply,
+// cannot make that first call mid-run.  This variant takes its scratch from a fixed array in the
+// static device memory of this module, which the CUDA runtime places when it loads the module,
+// and copies its one result word to the caller's host double.
+//
+// Scratch: NA_MAX_PARTIALS block maxima followed by the result word.  Pass 1 gives each block
+// NA_CHUNK consecutive cells and writes one partial maximum per block; pass 2 (one block) folds
+// partials [0, blocks) into the result word.  Nothing in the scratch has to start at zero: every
+// slot that is read was written earlier in the same call.  The limit is therefore
+// NA_MAX_PARTIALS * NA_CHUNK cells; larger fields are rejected.  All calls on one device share the
+// array, so calls whose work overlaps on the device (other streams, other host threads) race.
+namespace mm {
+namespace {
+constexpr int NA_MAX_PARTIALS = 65536;  // 512 KiB of partials (+ the result word)
+constexpr int NA_CHUNK = TPB * 16;      // cells per pass-1 block: limit 268,435,456 cells
+constexpr int NA_FINAL_THREADS = 1024;
+constexpr int NA_MAX_DEVICES = 64;
+} // namespace
+} // namespace mm
+
+static __device__ __align__(256) double g_na_scratch[mm::NA_MAX_PARTIALS + 1];
+
+namespace mm {
+namespace {
+
+// Block-wide max (NaN wins) of a non-negative value, returned to thread 0 of a 1-D block.
+__device__ __forceinline__ double na_block_max(double v)
+{
+	__shared__ double red[32];
+	v = warp_max(v);
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	if (lane == 0) red[wid] = v;
+	__syncthreads();
+	if (wid == 0) {
+		const int nw = blockDim.x >> 5;
+		v = warp_max(lane < nw ? red[lane] : 0.0);
+	}
+	return v;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_scaled_abs_max_partials(size_t n, const T *__restrict__ M,
+                                                                 const T *__restrict__ s,
+                                                                 double *__restrict__ partials)
+{
+	const size_t base = (size_t)blockIdx.x * NA_CHUNK;
+	const size_t end = n - base < (size_t)NA_CHUNK ? n : base + NA_CHUNK;
+	double best = 0.0;
+	for (size_t i = base + threadIdx.x; i < end; i += TPB) {
+		const double si = (double)s[i];
+		if (si == 0.0) continue;
+		const double mx = M[i], my = M[i + n], mz = M[i + 2 * n];
+		best = fmax(best, (mx * mx + my * my + mz * mz) / (si * si));
+	}
+	best = na_block_max(best);
+	if (threadIdx.x == 0) partials[blockIdx.x] = best;
+}
+
+__global__ void __launch_bounds__(NA_FINAL_THREADS) k_scaled_abs_max_final(int blocks, double *scratch)
+{
+	double best = 0.0;
+	for (int i = threadIdx.x; i < blocks; i += NA_FINAL_THREADS) best = nan_max(best, scratch[i]);
+	best = na_block_max(best);
+	if (threadIdx.x == 0) scratch[NA_MAX_PARTIALS] = best;
+}
+
+// Device address of g_na_scratch on the current device, looked up once per device.
+mm_status na_scratch(double **out)
+{
+	static std::mutex mu;
+	static double *addr[NA_MAX_DEVICES] = {};
+	int dev = 0;
+	MM_CUDA(cudaGetDevice(&dev));
+	if (dev < 0 || dev >= NA_MAX_DEVICES)
+		return fail(MM_ERR_UNSUPPORTED, "mm_scaled_abs_max_noalloc: device index " + std::to_string(dev) +
+		                                    " beyond the " + std::to_string(NA_MAX_DEVICES) + " supported");
+	std::lock_guard<std::mutex> lock(mu);
+	if (!addr[dev]) {
+		double *ptr = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress((void **)&ptr, g_na_scratch);
+		if (e != cudaSuccess || !ptr)
+			return fail(MM_ERR_CUDA, std::string("mm_scaled_abs_max_noalloc: cudaGetSymbolAddress of the "
+			                                     "static scratch failed: ") + cudaGetErrorString(e));
+		addr[dev] = ptr;
+	}
+	*out = addr[dev];
+	return MM_OK;
+}
+
+} // namespace
+} // namespace mm
+
+extern "C" {
+
+MM_API mm_status mm_scaled_abs_max_noalloc(int prec, size_t n, const void *M, const void *scale,
+                                           double *result_host, void *stream)
+{
+	if (bad_prec(prec) || n == 0 || !M || !scale || !result_host)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_scaled_abs_max_noalloc: invalid argument");
+	const size_t blocks = (n + NA_CHUNK - 1) / NA_CHUNK;
+	if (blocks > (size_t)NA_MAX_PARTIALS)
+		return fail(MM_ERR_INVALID_ARGUMENT,
+		            "mm_scaled_abs_max_noalloc: n = " + std::to_string(n) + " cells exceeds its limit of " +
+		                std::to_string((size_t)NA_MAX_PARTIALS * NA_CHUNK) + " cells (static scratch of " +
+		                std::to_string(NA_MAX_PARTIALS) + " partial maxima of " + std::to_string(NA_CHUNK) +
+		                " cells each); use mm_scaled_abs_max");
+	double *scr = nullptr;
+	MM_TRY(na_scratch(&scr));
+	cudaStream_t st = as_stream(stream);
+	if (prec == MM_F64)
+		k_scaled_abs_max_partials<double><<<(unsigned)blocks, TPB, 0, st>>>(n, (const double *)M,
+		                                                                    (const double *)scale, scr);
+	else
+		k_scaled_abs_max_partials<float><<<(unsigned)blocks, TPB, 0, st>>>(n, (const float *)M,
+		                                                                   (const float *)scale, scr);
+	MM_TRY(after_launch("k_scaled_abs_max_partials"));
+	k_scaled_abs_max_final<<<1, NA_FINAL_THREADS, 0, st>>>((int)blocks, scr);
+	MM_TRY(after_launch("k_scaled_abs_max_final"));
+	double r = 0.0;
+	MM_CUDA(cudaMemcpyAsync(&r, scr + NA_MAX_PARTIALS, sizeof(double), cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	*result_host = sqrt(r);
+	return MM_OK;
 }
 
 } // extern "C"

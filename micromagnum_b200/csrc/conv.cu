@@ -562,6 +562,79 @@ __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> 
 	}
 }
 
+// ---- z pass in registers ------------------------------------------------------------------------
+// One thread per (kx, component, ky) column holds the whole length-PZ column in registers: the
+// forward DFT (upper half zero padding, nz <= PZ/2), the tensor multiply through shared memory,
+// and the inverse DFT, of which only the outputs z < nz are formed and stored.  A block covers
+// 32 consecutive kx (one warp per component and row: coalesced 256-byte loads and stores) and the
+// ky pair {b, py - b}, b = blockIdx.y <= py/2, whose tensor entries agree up to parity signs: each
+// tensor value is read once per block and applied to up to four (ky, kz) combinations.
+constexpr int ZR_THREADS = 192;  // 32 kx x 3 components x 2 rows
+
+template <typename T, int PZ>
+__global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
+                                                        int py, int hx, int qy, int qz)
+{
+	using C = cplx<T>;
+	constexpr int H = PZ / 2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *sm = reinterpret_cast<C *>(smem_raw);  // [row][kz][component][32 kx]
+	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+	const int c = w % 3, r = w / 3;
+	const int b = blockIdx.y, b1 = py - b;
+	const bool two = b > 0 && b1 != b;
+	const int kx = blockIdx.x * 32 + lane;
+	const bool ok = (r == 0 || two) && kx < hx;
+	const size_t zstride = (size_t)py * hx;
+	C *col = S + ((size_t)c * nz * py + (size_t)(r == 0 ? b : b1)) * hx + kx;
+	C v[PZ];
+#pragma unroll
+	for (int z = 0; z < H; ++z) v[z] = (ok && z < nz) ? col[z * zstride] : C{0, 0};
+	dft_reg_halfzero<T, PZ>(v);
+	C *mine = sm + (r * PZ * 3 + c) * 32 + lane;
+#pragma unroll
+	for (int k = 0; k < PZ; ++k) mine[brev<PZ>(k) * 96] = v[k];
+	__syncthreads();
+	if (kx < hx) {
+		const size_t cs = (size_t)qz * qy * hx, kzs = (size_t)qy * hx;
+		const T *tb = Nt + (size_t)b * hx + kx;
+		for (int kzr = w; kzr <= H; kzr += ZR_THREADS / 32) {
+			const T *t = tb + kzr * kzs;
+			const T nxx = t[0], nxy = t[cs], nxz = t[2 * cs], nyy = t[3 * cs], nyz = t[4 * cs], nzz = t[5 * cs];
+			const int nk = (kzr == 0 || kzr == H) ? 1 : 2;
+			for (int rr = 0; rr < (two ? 2 : 1); ++rr) {
+				for (int q = 0; q < nk; ++q) {
+					const int kz = q ? PZ - kzr : kzr;
+					const T sy = rr ? T(-1) : T(1), sz = q ? T(-1) : T(1);
+					C *e = sm + ((rr * PZ + kz) * 3) * 32 + lane;
+					const C m0 = e[0], m1 = e[32], m2 = e[64];
+					const T xy = sy * nxy, xz = sz * nxz, yz = sy * sz * nyz;
+					e[0] = C{nxx * m0.x + xy * m1.x + xz * m2.x, nxx * m0.y + xy * m1.y + xz * m2.y};
+					e[32] = C{xy * m0.x + nyy * m1.x + yz * m2.x, xy * m0.y + nyy * m1.y + yz * m2.y};
+					e[64] = C{xz * m0.x + yz * m1.x + nzz * m2.x, xz * m0.y + yz * m1.y + nzz * m2.y};
+				}
+			}
+		}
+	}
+	__syncthreads();
+#pragma unroll
+	for (int k = 0; k < PZ; ++k) v[k] = mine[k * 96];
+	dft_reg<T, PZ, true>(v);
+	if (ok) {
+#pragma unroll
+		for (int z = 0; z < H; ++z)
+			if (z < nz) col[z * zstride] = v[brev<PZ>(z)];
+	}
+}
+
+template <typename T, int PZ>
+void fs_z_reg(ConvPlan *p, cudaStream_t st)
+{
+	const dim3 grid((p->hx + 31) / 32, p->qy);
+	k_z_reg<T, PZ><<<grid, ZR_THREADS, (size_t)2 * PZ * 96 * sizeof(cplx<T>), st>>>(
+	    (cplx<T> *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz);
+}
+
 // ---- fast-path geometry and dispatch ---------------------------------------------------------------
 
 
@@ -661,7 +734,17 @@ mm_status fs_setup(ConvPlan *p)
 	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_SETUP); MM_TRY(r); }
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_SETUP); MM_TRY(r); }
 #undef MM_SETUP
-	if (p->fast_z) {
+	p->reg_z = p->fast_z && 2 * p->nz <= p->pz && p->pz <= (sizeof(T) == 4 ? 32 : 16);
+	if (p->reg_z) {
+		const size_t sz = (size_t)2 * p->pz * 96 * sizeof(cplx<T>);
+		switch (p->pz) {
+		case 2: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 2>, sz)); break;
+		case 4: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 4>, sz)); break;
+		case 8: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 8>, sz)); break;
+		case 16: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 16>, sz)); break;
+		case 32: if constexpr (sizeof(T) == 4) { MM_TRY(set_smem<T>((const void *)k_z_reg<T, 32>, sz)); } break;
+		}
+	} else if (p->fast_z) {
 		const size_t sz = (size_t)(p->pz * 3 * CT_ZTB + (p->pz * 3 * CT_ZTB >> 5) + 1) * sizeof(cplx<T>);
 		switch (p->pz) {
 		case 2: MM_TRY(set_smem<T>((const void *)k_z_ct<T, 2, CT_ZTB>, sz)); break;
@@ -822,7 +905,15 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		prof_end(tk, "k_y_fwd", half + ypad, st);
 		dim3 gz((p->hx + p->tb_z - 1) / p->tb_z, p->py, 1);
 		tk = prof_begin(st);
-		if (p->fast_z) {
+		if (p->reg_z) {
+			switch (p->pz) {
+			case 2: fs_z_reg<T, 2>(p, st); break;
+			case 4: fs_z_reg<T, 4>(p, st); break;
+			case 8: fs_z_reg<T, 8>(p, st); break;
+			case 16: fs_z_reg<T, 16>(p, st); break;
+			case 32: if constexpr (sizeof(T) == 4) { fs_z_reg<T, 32>(p, st); } break;
+			}
+		} else if (p->fast_z) {
 			switch (p->pz) {
 			case 2: fs_z<T, 2>(p, st); break;
 			case 4: fs_z<T, 4>(p, st); break;

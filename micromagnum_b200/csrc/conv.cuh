@@ -14,6 +14,7 @@ struct ConvPlan {
 	int qy = 0, qz = 0;             // py/2 + 1, pz/2 + 1 stored tensor frequencies
 	bool is2d = false;              // nz == 1 && pz == 1
 	bool fast_x = false, fast_y = false, fast_z = false;  // power-of-two register-FFT passes
+	bool reg_z = false;             // z pass with whole columns in registers (nz <= pz/2, pz small)
 	FftRadices rx{}, ry{}, rz{};
 	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
 	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]

@@ -39,12 +39,13 @@ __host__ __device__ constexpr int brev_c(int k, int n)
 template <int N>
 __device__ __forceinline__ int brev(int k) { return brev_c(k, N); }
 
-template <typename T, int N, bool INV>
-__device__ __forceinline__ void dft_reg(cplx<T> (&v)[N])
+// Radix-2 DIF stages of span SPAN0, SPAN0/2, ..., 1 over v[0..N) (the full DFT has SPAN0 = N/2).
+template <typename T, int N, bool INV, int SPAN0>
+__device__ __forceinline__ void dif_stages(cplx<T> (&v)[N])
 {
 	using C = cplx<T>;
 #pragma unroll
-	for (int span = N / 2; span >= 1; span >>= 1) {
+	for (int span = SPAN0; span >= 1; span >>= 1) {
 #pragma unroll
 		for (int b = 0; b < N; b += 2 * span) {
 #pragma unroll
@@ -63,6 +64,29 @@ __device__ __forceinline__ void dft_reg(cplx<T> (&v)[N])
 				v[b + j + span] = d;
 			}
 		}
+	}
+}
+
+template <typename T, int N, bool INV>
+__device__ __forceinline__ void dft_reg(cplx<T> (&v)[N])
+{
+	dif_stages<T, N, INV, N / 2>(v);
+}
+
+// Forward DFT of a column whose upper half v[N/2..N) is zero padding: the first DIF stage reduces
+// to v[j + N/2] = v[j] W_N^j.  Output in bit-reversed order, like dft_reg.
+template <typename T, int N>
+__device__ __forceinline__ void dft_reg_halfzero(cplx<T> (&v)[N])
+{
+	if constexpr (N >= 2) {
+#pragma unroll
+		for (int j = 0; j < N / 2; ++j) {
+			const int q = j * (64 / N);
+			if (q == 0) v[j + N / 2] = v[j];
+			else if (q == 16) v[j + N / 2] = mul_mi<false>(v[j]);
+			else v[j + N / 2] = cmul(v[j], w64<T>(q));
+		}
+		dif_stages<T, N, false, N / 4>(v);
 	}
 }
 

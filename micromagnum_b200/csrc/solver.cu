@@ -274,89 +274,97 @@ struct StageCoef {
 
 // One fused stage: k_i = f(y_in) (demag field from Hd), then the next stage state
 // y_{i+1} = y_n + h sum_{l<=i} b_{i+1,l} k_l, or on the last stage the error maximum and y_{n+1}.
-// COMP: compensated float state (y_n = yhi + ylo).  Each thread handles CPT cells 32 apart in x
-// (every warp access stays a contiguous 128-byte run) and issues all their loads before any
-// store, so twice the bytes are in flight per thread.
+// COMP: compensated float state (y_n = yhi + ylo).  S = i is a template argument, so the sums
+// over earlier stages unroll and their loads issue together.  The grid is persistent: each block
+// loads the Ms table once and walks tiles of 32*STAGE_CPT x 8 cells; each thread handles CPT
+// cells 32 apart in x (every warp access stays a contiguous 128-byte run) and issues all their
+// loads before any store, so twice the bytes are in flight per thread.
 constexpr int STAGE_CPT = 2;
+template <typename T>
+constexpr int stage_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }  // FP64 needs ~126 registers
 
-template <typename T, bool COMP>
-__global__ void __launch_bounds__(256) k_stage(CellArgs<T> a, StageCoef sc,
-                                               const T *__restrict__ y_in, const T *__restrict__ Hd,
-                                               const T *__restrict__ yhi, const T *__restrict__ ylo,
-                                               const KTab<T> *__restrict__ ktab, T *__restrict__ y_out,
-                                               T *__restrict__ y_out_lo, const DevState *__restrict__ st,
-                                               double *red_err, double *red_k0)
+template <typename T, bool COMP, int S>
+__global__ void __launch_bounds__(256, stage_min_blocks<T>())
+    k_stage(CellArgs<T> a, StageCoef sc, const T *__restrict__ y_in, const T *__restrict__ Hd,
+            const T *__restrict__ yhi, const T *__restrict__ ylo, const KTab<T> *__restrict__ ktab,
+            T *__restrict__ y_out, T *__restrict__ y_out_lo, const DevState *__restrict__ st, double *red_err,
+            double *red_k0, int tiles_x, int tiles_y, int ntiles)
 {
 	__shared__ T msr[256];
 	load_ms_table(a, msr);
-	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
-	const int z = blockIdx.z;
 	const size_t n = (size_t)a.nx * a.ny * a.nz;
 	const double h = st->h;
 	const double t = st->t + sc.a_i * h;
 	T *const *K = ktab->k;
-	V3<T> ki[STAGE_CPT];
-	size_t idx[STAGE_CPT];
-	bool in[STAGE_CPT];
-#pragma unroll
-	for (int u = 0; u < STAGE_CPT; ++u) {
-		const int x = blockIdx.x * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
-		in[u] = x < a.nx && yy < a.ny;
-		idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
-		if (in[u]) {
-			V3<T> Heff;
-			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
-			cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
-		}
-	}
 	T e2 = T(0), k02 = T(0);
+	for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+		const int tx = tile % tiles_x, rest = tile / tiles_x;
+		const int yy = (rest % tiles_y) * blockDim.y + threadIdx.y;
+		const int z = rest / tiles_y;
+		V3<T> ki[STAGE_CPT];
+		size_t idx[STAGE_CPT];
+		bool in[STAGE_CPT];
 #pragma unroll
-	for (int u = 0; u < STAGE_CPT; ++u) {
-		if (!in[u]) continue;
-		const size_t i = idx[u];
-		if (!sc.last) {
-			if (sc.write_next) {
-				V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
-				for (int l = 0; l < sc.stage; ++l) {
-					const T f = (T)(h * sc.bn[l]);
-					if (f != T(0)) acc = acc + f * load3(K[l], i, n);
-				}
-				acc = acc + (T)(h * sc.bn[sc.stage]) * ki[u];
-				if (COMP) acc = load3(yhi, i, n) + acc;
-				store3(y_out, i, n, acc);
-			}
-			if (sc.reduce_k0) {
-				const V3<T> k0 = sc.stage == 0 ? ki[u] : load3(K[0], i, n);
-				k02 = max(k02, dot(k0, k0));
-			}
-		} else {
-			V3<T> err = v3<T>(0, 0, 0);
-			V3<T> acc = v3<T>(0, 0, 0);
-			for (int l = 0; l <= sc.stage; ++l) {
-				const T fe = (T)(h * sc.ec[l]);
-				const T fc = (T)(h * sc.bn[l]);
-				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
-				const V3<T> kl = l == sc.stage ? ki[u] : load3(K[l], i, n);
-				err = err + fe * kl;
-				if (sc.write_new) acc = acc + fc * kl;
-			}
-			e2 = nan_max(e2, dot(err, err));
-			if (sc.write_new) {
-				if (COMP) {
-					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
-					const V3<T> hi = load3(yhi, i, n);
-					const V3<T> d = load3(ylo, i, n) + acc;
-					const V3<T> s = hi + d;
-					const V3<T> bb = s - hi;
-					const V3<T> lo = (hi - (s - bb)) + (d - bb);
-					store3(y_out, i, n, s);
-					store3(y_out_lo, i, n, lo);
-				} else {
-					store3(y_out, i, n, load3(yhi, i, n) + acc);
-				}
+		for (int u = 0; u < STAGE_CPT; ++u) {
+			const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
+			in[u] = x < a.nx && yy < a.ny;
+			idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
+			if (in[u]) {
+				V3<T> Heff;
+				const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
+				cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
 			}
 		}
-		store3(K[sc.stage], i, n, ki[u]);
+#pragma unroll
+		for (int u = 0; u < STAGE_CPT; ++u) {
+			if (!in[u]) continue;
+			const size_t i = idx[u];
+			if (!sc.last) {
+				if (sc.write_next) {
+					V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
+#pragma unroll
+					for (int l = 0; l < S; ++l) {
+						const T f = (T)(h * sc.bn[l]);
+						if (f != T(0)) acc = acc + f * load3(K[l], i, n);
+					}
+					acc = acc + (T)(h * sc.bn[S]) * ki[u];
+					if (COMP) acc = load3(yhi, i, n) + acc;
+					store3(y_out, i, n, acc);
+				}
+				if (sc.reduce_k0) {
+					const V3<T> k0 = S == 0 ? ki[u] : load3(K[0], i, n);
+					k02 = max(k02, dot(k0, k0));
+				}
+			} else {
+				V3<T> err = v3<T>(0, 0, 0);
+				V3<T> acc = v3<T>(0, 0, 0);
+#pragma unroll
+				for (int l = 0; l <= S; ++l) {
+					const T fe = (T)(h * sc.ec[l]);
+					const T fc = (T)(h * sc.bn[l]);
+					if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
+					const V3<T> kl = l == S ? ki[u] : load3(K[l], i, n);
+					err = err + fe * kl;
+					if (sc.write_new) acc = acc + fc * kl;
+				}
+				e2 = nan_max(e2, dot(err, err));
+				if (sc.write_new) {
+					if (COMP) {
+						// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
+						const V3<T> hi = load3(yhi, i, n);
+						const V3<T> d = load3(ylo, i, n) + acc;
+						const V3<T> s = hi + d;
+						const V3<T> bb = s - hi;
+						const V3<T> lo = (hi - (s - bb)) + (d - bb);
+						store3(y_out, i, n, s);
+						store3(y_out_lo, i, n, lo);
+					} else {
+						store3(y_out, i, n, load3(yhi, i, n) + acc);
+					}
+				}
+			}
+			store3(K[S], i, n, ki[u]);
+		}
 	}
 	if (sc.last) block_max_to(red_err, e2);
 	if (sc.reduce_k0) block_max_to(red_k0, k02);
@@ -699,6 +707,55 @@ double stage_bytes(const mm_solver *s, const StageCoef &sc)
 	return b;
 }
 
+// Resident blocks of the fused stage kernel on the whole device (occupancy of the S = 6 instance),
+// looked up once; solver creation calls it so that no later call does so during stream capture.
+template <typename T, bool COMP>
+int stage_resident()
+{
+	static const int resident = [] {
+		int per_sm = 0;
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<T, COMP, 6>, 256, 0) != cudaSuccess ||
+		    per_sm < 1) {
+			cudaGetLastError();
+			per_sm = stage_min_blocks<T>();
+		}
+		return per_sm * num_sms();
+	}();
+	return resident;
+}
+
+// Launches the fused stage kernel for stage S on a persistent grid of at most the resident blocks.
+template <typename T, bool COMP, int S>
+void stage_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc, const T *yin, const T *yhi,
+                  const T *ylo, const KTab<T> *kt, T *yout, DevState *ds, cudaStream_t st)
+{
+	const int resident = stage_resident<T, COMP>();
+	const dim3 tg = stage_grid(s->cfg);
+	const int ntiles = (int)(tg.x * tg.y * tg.z);
+	const int grid = ntiles < resident ? ntiles : resident;
+	k_stage<T, COMP, S><<<grid, dim3(32, 8, 1), 0, st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, yout,
+	                                                     (T *)s->ynew_lo, ds, &ds->max_err2, &ds->max_k02,
+	                                                     (int)tg.x, (int)tg.y, ntiles);
+}
+
+template <typename T, bool COMP>
+mm_status launch_stage(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc, const T *yin, const T *yhi,
+                       const T *ylo, const KTab<T> *kt, T *yout, DevState *ds, cudaStream_t st)
+{
+	switch (sc.stage) {
+	case 0: stage_launch<T, COMP, 0>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 1: stage_launch<T, COMP, 1>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 2: stage_launch<T, COMP, 2>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 3: stage_launch<T, COMP, 3>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 4: stage_launch<T, COMP, 4>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 5: stage_launch<T, COMP, 5>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 6: stage_launch<T, COMP, 6>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	case 7: stage_launch<T, COMP, 7>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+	default: return fail(MM_ERR_INVALID_ARGUMENT, "stage index beyond the supported tableau size");
+	}
+	return after_launch("k_stage");
+}
+
 // y_1 = y_n + h b_10 k_0 when k_0 is the previous attempt's last stage (first same as last).
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(256) k_prepare1(size_t n3, double b10, const T *__restrict__ yhi,
@@ -724,9 +781,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 	constexpr bool COMP = sizeof(T) == 4;
 	const Tableau &tb = s->tab;
 	const CellArgs<T> &a = args_of<T>(s);
-	const dim3 grid = stage_grid(s->cfg), block(32, 8, 1);
 	DevState *ds = s->dst;
-	double *red_err = &ds->max_err2, *red_k0 = &ds->max_k02;
 	const T *yhi = (const T *)s->m, *ylo = (const T *)s->m_lo;
 	const KTab<T> *kt = (const KTab<T> *)s->ktab;
 	T *ys[2] = {(T *)s->ys[0], (T *)s->ys[1]};
@@ -738,9 +793,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		sc.bn[0] = tb.b[1][0];
 		MM_TRY(demag<T>(s, s->m, st));
 		ProfToken tk = prof_begin(st);
-		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yhi, (const T *)s->hd, yhi, ylo, kt, ys[0],
-		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
-		MM_TRY(after_launch("k_stage"));
+		MM_TRY((launch_stage<T, COMP>(s, a, sc, yhi, yhi, ylo, kt, ys[0], ds, st)));
 		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
 	} else {
 		const size_t n3 = 3 * s->n;
@@ -768,9 +821,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		const T *yin = ys[(i - 1) & 1];
 		MM_TRY(demag<T>(s, yin, st));
 		ProfToken tk = prof_begin(st);
-		k_stage<T, COMP><<<grid, block, 0, st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, ys[i & 1],
-		                                         (T *)s->ynew_lo, ds, red_err, red_k0);
-		MM_TRY(after_launch("k_stage"));
+		MM_TRY((launch_stage<T, COMP>(s, a, sc, yin, yhi, ylo, kt, ys[i & 1], ds, st)));
 		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
 		if (sc.last) s->last_stage_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
 	}
@@ -988,6 +1039,7 @@ mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uin
 		if (N) cudaFree(N);
 		MM_TRY(r);
 	}
+	stage_resident<T, sizeof(T) == 4>();
 	MM_CUDA(cudaStreamSynchronize(st));
 	return MM_OK;
 }

@@ -285,6 +285,24 @@ MM_API mm_status mm_solver_eval(mm_solver *s, double *H_eff_device, double *dMdt
 
 MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *stream);
 
+/* Relaxation norms of the current state (one RHS evaluation): norms_host3[0] = max |dM/dt|
+ * [A/(m s)] (state.dMdt.absMax()), [1] = max |M| [A/m] (state.M.absMax()), [2] = max over cells
+ * with Ms != 0 of |m x H_eff| / Ms (dimensionless torque).  Synchronises `stream`. */
+MM_API mm_status mm_solver_relax_norms(mm_solver *s, double *norms_host3, void *stream);
+
+enum { MM_RELAX_DEG_PER_NS = 0, MM_RELAX_TORQUE = 1 };
+
+/* Steps (t_max = 1e100, like Solver.solve with a condition that has no time of interest) until
+ * the state is relaxed, checking every check_every_nth_step-th step (state.step % n == 0).
+ * MM_RELAX_DEG_PER_NS replaces condition.Relaxed(max_degree_per_ns = threshold,
+ * check_every_nth_step) (magnum/solver/condition.py:169-200, deg_per_ns from
+ * landau_lifshitz_gilbert.py:127-131): relaxed when deg/ns <= threshold and smaller than at the
+ * previous check of this call.  MM_RELAX_TORQUE: relaxed when max |m x H_eff| / Ms < threshold
+ * (no reference counterpart; the batched-relaxation criterion).  max_steps < 0: no limit.
+ * *relaxed = 1 when the criterion was met; *last_value (optional) = the last deg/ns or torque. */
+MM_API mm_status mm_solver_relax(mm_solver *s, int criterion, double threshold, int check_every_nth_step,
+                                 long long max_steps, int *relaxed, double *last_value, void *stream);
+
 /* <M> [A/m] averaged over all cells (VectorMatrix::average). Synchronises `stream`. */
 MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg_host3, void *stream);
 

@@ -21,6 +21,7 @@ MM_F64, MM_F32 = 0, 1
 MM_RK_RKF45, MM_RK_CC45, MM_RK_DP54, MM_RK_RK23 = 0, 1, 2, 3
 MM_TERM_DEMAG, MM_TERM_EXCHANGE, MM_TERM_UNIAXIAL = 1, 2, 4
 MM_TERM_CUBIC, MM_TERM_ZHANGLI, MM_TERM_ZEEMAN = 8, 16, 32
+MM_RELAX_DEG_PER_NS, MM_RELAX_TORQUE = 0, 1
 
 
 class MMError(RuntimeError):
@@ -100,6 +101,8 @@ _PROTOS = [
     ("mm_solver_eval", _I, [_VP, _VP, _VP, _VP, _VP]),
     ("mm_solver_stats_get", _I, [_VP, ctypes.POINTER(mm_solver_stats), _VP]),
     ("mm_solver_average_M", _I, [_VP, _DP, _VP]),
+    ("mm_solver_relax_norms", _I, [_VP, _DP, _VP]),
+    ("mm_solver_relax", _I, [_VP, _I, _D, _I, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int), _DP, _VP]),
 ]
 
 EXPORTED = [p[0] for p in _PROTOS]

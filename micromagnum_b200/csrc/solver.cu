@@ -462,6 +462,41 @@ __global__ void __launch_bounds__(256) k_eval(CellArgs<T> a, const T *__restrict
 	if (Hd_out) { Hd_out[i] = hd.x; Hd_out[i + n] = hd.y; Hd_out[i + 2 * n] = hd.z; }
 }
 
+// Relaxation norms of the current state, reduced into red[0..2]: max |dM/dt|^2 [(A/(m s))^2],
+// max |M|^2 [(A/m)^2] (VectorMatrix::absMax, squared) and max (|m x H_eff| / Ms)^2 over cells
+// with Ms != 0 (the torque criterion of batched relaxations).
+template <typename T>
+__global__ void __launch_bounds__(256) k_relax_norms(CellArgs<T> a, const T *__restrict__ m,
+                                                     const T *__restrict__ Hd, double t, double *red)
+{
+	__shared__ T msr[256];
+	load_ms_table(a, msr);
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	double dm2 = 0.0, M2 = 0.0, tq2 = 0.0;
+	if (x < a.nx && yy < a.ny) {
+		const size_t n = (size_t)a.nx * a.ny * a.nz;
+		const size_t i = ((size_t)z * a.ny + yy) * a.nx + x;
+		V3<T> Heff, dm;
+		const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, i, n) : v3<T>(0, 0, 0);
+		cell_rhs<T>(a, msr, m, n, x, yy, z, i, hd, t, Heff, dm);
+		const double ms = (double)mat_of(a, i).Ms;
+		if (ms != 0.0) {
+			const V3<T> mi = load3(m, i, n);
+			const double mx = mi.x, my = mi.y, mz = mi.z;
+			const double hx = Heff.x, hy = Heff.y, hz = Heff.z;
+			const double cx = my * hz - mz * hy, cy = mz * hx - mx * hz, cz = mx * hy - my * hx;
+			dm2 = ms * ms * ((double)dm.x * dm.x + (double)dm.y * dm.y + (double)dm.z * dm.z);
+			M2 = ms * ms * (mx * mx + my * my + mz * mz);
+			tq2 = (cx * cx + cy * cy + cz * cz) / (ms * ms);
+		}
+	}
+	block_max_to(red, dm2);
+	block_max_to(red + 1, M2);
+	block_max_to(red + 2, tq2);
+}
+
 // M (A/m, FP64) -> unit state, normalised (LandauLifshitzGilbert.update("M")).
 template <typename T, bool COMP>
 __global__ void k_set_M(size_t n, const double *__restrict__ M, const uint8_t *__restrict__ reg,
@@ -983,6 +1018,21 @@ mm_status average(mm_solver *s, double *out3, cudaStream_t st)
 	return MM_OK;
 }
 
+// Relaxation norms (square roots of k_relax_norms' maxima) of the current state; synchronises.
+template <typename T>
+mm_status relax_norms(mm_solver *s, double out3[3], cudaStream_t st)
+{
+	MM_TRY(demag<T>(s, s->m, st));
+	MM_CUDA(cudaMemsetAsync(s->avg, 0, 3 * sizeof(double), st));
+	k_relax_norms<T><<<cell_grid(s->cfg), dim3(32, 8, 1), 0, st>>>(args_of<T>(s), (const T *)s->m,
+	                                                               (const T *)s->hd, s->t, s->avg);
+	MM_TRY(after_launch("k_relax_norms"));
+	MM_CUDA(cudaMemcpyAsync(s->avg_h, s->avg, 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	for (int c = 0; c < 3; ++c) out3[c] = sqrt(s->avg_h[c]);
+	return MM_OK;
+}
+
 void free_solver(mm_solver *s)
 {
 	if (!s) return;
@@ -1232,6 +1282,50 @@ MM_API mm_status mm_solver_eval(mm_solver *s, double *H_eff, double *dMdt, doubl
 		                                      dMdt, H_demag);
 	}
 	return after_launch("k_eval");
+}
+
+MM_API mm_status mm_solver_relax_norms(mm_solver *s, double *norms_host3, void *stream)
+{
+	if (!s || !norms_host3) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_relax_norms: null argument");
+	cudaStream_t st = as_stream(stream);
+	return s->cfg.precision == MM_F64 ? relax_norms<double>(s, norms_host3, st) : relax_norms<float>(s, norms_host3, st);
+}
+
+MM_API mm_status mm_solver_relax(mm_solver *s, int criterion, double threshold, int check_every_nth_step,
+                                 long long max_steps, int *relaxed, double *last_value, void *stream)
+{
+	if (!s || !relaxed || check_every_nth_step < 1 || !(threshold > 0) ||
+	    (criterion != MM_RELAX_DEG_PER_NS && criterion != MM_RELAX_TORQUE))
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_relax: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	const bool f64 = s->cfg.precision == MM_F64;
+	*relaxed = 0;
+	bool have_last = false;
+	double last = 0.0;
+	for (long long taken = 0;; ++taken) {
+		// condition.Relaxed.check (condition.py:178-199): only every nth step
+		if (s->steps % check_every_nth_step == 0) {
+			double nrm[3];
+			MM_TRY(f64 ? relax_norms<double>(s, nrm, st) : relax_norms<float>(s, nrm, st));
+			if (criterion == MM_RELAX_DEG_PER_NS) {
+				// LandauLifshitzGilbert.calculate_deg_per_ns (landau_lifshitz_gilbert.py:127-131)
+				const double deg_per_step = (180.0 / M_PI) * atan2(nrm[0] * s->h, nrm[1]);
+				const double deg_per_ns = 1e-9 * deg_per_step / s->h;
+				const bool done = have_last && deg_per_ns < last && deg_per_ns <= threshold;
+				last = deg_per_ns;
+				have_last = true;
+				if (done) { *relaxed = 1; break; }
+			} else {
+				last = nrm[2];
+				if (nrm[2] < threshold) { *relaxed = 1; break; }
+			}
+		}
+		if (max_steps >= 0 && taken >= max_steps) break;
+		MM_TRY(f64 ? evolve<double>(s, 1e100, st) : evolve<float>(s, 1e100, st));
+	}
+	if (last_value) *last_value = last;
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
 }
 
 MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *stream)

@@ -10,6 +10,7 @@ reference's semantics (runge_kutta.py:47-137, micro_magnetics_stepsize_controlle
 from __future__ import annotations
 
 import ctypes
+import math
 from dataclasses import dataclass, field
 from typing import Iterable, Optional, Sequence
 
@@ -207,6 +208,40 @@ class Solver:
         out = (ctypes.c_double * 3)()
         check(lib().mm_solver_average_M(self._h, out, _stream_ptr()))
         return tuple(out)
+
+    def relax_norms(self):
+        """(max |dM/dt| [A/(m s)], max |M| [A/m], max |m x H_eff| / Ms) at the current state."""
+        out = (ctypes.c_double * 3)()
+        check(lib().mm_solver_relax_norms(self._h, out, _stream_ptr()))
+        return tuple(out)
+
+    @property
+    def deg_per_ns(self) -> float:
+        """LandauLifshitzGilbert.calculate_deg_per_ns (landau_lifshitz_gilbert.py:127-131) with the
+        last step size."""
+        dmdt, m, _ = self.relax_norms()
+        h = self.stats["h"]
+        return 1e-9 * math.degrees(math.atan2(dmdt * h, m)) / h
+
+    def relax(self, max_degree_per_ns: float = 1.0, check_every_nth_step: int = 100,
+              max_steps: Optional[int] = None) -> bool:
+        """Solver.solve(condition.Relaxed(max_degree_per_ns, check_every_nth_step))
+        (condition.py:169-200); returns True when relaxed (False when max_steps ran out)."""
+        return self._relax(_lib.MM_RELAX_DEG_PER_NS, max_degree_per_ns, check_every_nth_step, max_steps)
+
+    def relax_torque(self, max_torque: float = 1e-4, check_every_nth_step: int = 1,
+                     max_steps: Optional[int] = None) -> bool:
+        """Steps until max |m x H_eff| / Ms < max_torque (checked every nth step)."""
+        return self._relax(_lib.MM_RELAX_TORQUE, max_torque, check_every_nth_step, max_steps)
+
+    def _relax(self, criterion, threshold, every, max_steps):
+        done = ctypes.c_int(0)
+        last = ctypes.c_double(0.0)
+        check(lib().mm_solver_relax(self._h, criterion, float(threshold), int(every),
+                                    -1 if max_steps is None else int(max_steps), ctypes.byref(done),
+                                    ctypes.byref(last), _stream_ptr()))
+        self.last_relax_value = last.value
+        return bool(done.value)
 
     @property
     def stats(self) -> dict:

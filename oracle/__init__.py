@@ -14,6 +14,7 @@ N = nx*ny*nz, x fastest; the demag tensor is flat (ez, ey, ex, 6) == Matrix(Shap
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -305,6 +306,37 @@ class Solver:
         o = np.zeros(6)
         self.L.or_solver_stats(ctypes.c_void_p(self.h), _p(o))
         return dict(t=o[0], h=o[1], h_next=o[2], steps=int(o[3]), attempts=int(o[4]), rejected=int(o[5]))
+
+    def relax_norms(self):
+        """(state.dMdt.absMax(), state.M.absMax(), max |m x H| / Ms) at the current state."""
+        H, dM, _ = self.eval()
+        M = self.M
+        Ms = np.sqrt((M ** 2).sum(0))
+        m = np.divide(M, Ms, out=np.zeros_like(M), where=Ms > 0)
+        tq = np.sqrt((np.cross(m.T, H.T) ** 2).sum(1))
+        tq = np.divide(tq, Ms, out=np.zeros_like(tq), where=Ms > 0)
+        return float(np.sqrt((dM ** 2).sum(0)).max()), float(Ms.max()), float(tq.max())
+
+    def relax(self, max_degree_per_ns=1.0, check_every_nth_step=100, max_steps=None):
+        """Solver.solve(condition.Relaxed(...)) restated: condition.py:169-200 checks every nth
+        step (state.step % n == 0) and calls the state relaxed when deg/ns (from
+        landau_lifshitz_gilbert.py:127-131, with the last step size state.h) is <= the limit and
+        below its value at the previous check; solver.py:117-122 checks before each step.
+        Returns (relaxed, last deg/ns)."""
+        last, taken = None, 0
+        while True:
+            st = self.stats
+            if st["steps"] % check_every_nth_step == 0:
+                dmdt, mmax, _ = self.relax_norms()
+                deg = 1e-9 * math.degrees(math.atan2(dmdt * st["h"], mmax)) / st["h"]
+                done = last is not None and deg < last and deg <= max_degree_per_ns
+                last = deg
+                if done:
+                    return True, deg
+            if max_steps is not None and taken >= max_steps:
+                return False, last
+            self.step()
+            taken += 1
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -125,6 +125,16 @@ def test_trajectory_film(sv, oracle_mod, ref_available, prec, tol):
     orc.M = M
     t1, m1 = ours.solve(1e-10, sample_dt=1e-12)
     t2, m2 = orc.solve(1e-10, sample_dt=1e-12)
+    if prec == "f32":
+        # a step that ends one ulp short of a sample time is followed by a one-ulp step onto it, and
+        # condition.EveryNthSecond samples both (the reference's own tolerance test,
+        # condition.py:121-133); the FP32 step sequence may meet this where the FP64 one does not,
+        # so compare the last sample taken at each sample time
+        def last_per_time(t, m):
+            keep = np.append(np.abs(np.diff(t)) > 1e-20, True)
+            return t[keep], m[keep]
+        t1, m1 = last_per_time(t1, m1)
+        t2, m2 = last_per_time(t2, m2)
     assert len(t1) == len(t2) == 101
     assert np.allclose(t1, t2, rtol=1e-12, atol=0)
     err = np.abs(m1 - m2).max() / 8e5
@@ -183,3 +193,47 @@ def test_launch_counter_and_native_library(sv):
     s.M = (8e5, 0, 0)
     s.step()
     assert _lib.launches() > before
+
+
+def test_relaxed_condition_matches_oracle(sv, oracle_mod, ref_available):
+    # condition.Relaxed(max_degree_per_ns, check_every_nth_step) on the film from a random state:
+    # the same check steps, the same decision and the same final <M> as the oracle's restatement
+    if not ref_available:
+        pytest.skip("reference not built")
+    dims, delta = (32, 8, 1), (3.90625e-9, 3.90625e-9, 3e-9)
+    mats = [sv.Material(Ms=8e5, A=1.3e-11, alpha=0.5)]
+    kw = dict(evolver="dp54", eps_abs=1e-4, eps_rel=1e-4)
+    ours, orc = make_pair(sv, oracle_mod, dims, delta, mats, None, ("demag", "exchange"), "f64", **kw)
+    M = unit_random(np.random.default_rng(5), int(np.prod(dims))) * 8e5
+    ours.M = M
+    orc.M = M
+    # the norms behind deg/ns at the initial state agree with the oracle's
+    dmdt, mmax, tq = ours.relax_norms()
+    rd, rm, rt = orc.relax_norms()
+    assert dmdt == pytest.approx(rd, rel=1e-12) and mmax == pytest.approx(rm, rel=1e-12)
+    assert tq == pytest.approx(rt, rel=1e-12)
+    ok1 = ours.relax(max_degree_per_ns=2000.0, check_every_nth_step=20, max_steps=3000)
+    ok2, deg2 = orc.relax(max_degree_per_ns=2000.0, check_every_nth_step=20, max_steps=3000)
+    assert ok1 == ok2
+    assert ours.stats["steps"] == orc.stats["steps"]
+    assert ours.last_relax_value == pytest.approx(deg2, rel=1e-6)
+    assert np.abs(np.array(ours.average_M()) - orc.M.mean(1)).max() / 8e5 < 1e-6
+
+
+def test_torque_relaxation_criterion(sv, oracle_mod):
+    # relax_torque stops at the first checked step with max |m x H| / Ms below the threshold;
+    # the oracle's norms at the returned state confirm the value
+    dims, delta = (24, 12, 2), (4e-9, 4e-9, 4e-9)
+    n = int(np.prod(dims))
+    mats = [sv.Material(Ms=1e6, A=1.5e-11, alpha=0.5)]
+    s = sv.Solver(sv.RectangularMesh(dims, delta), mats, terms=("demag", "exchange"), precision="f64",
+                  evolver="dp54", eps_abs=1e-4, eps_rel=1e-4)
+    s.M = unit_random(np.random.default_rng(8), n) * 1e6
+    assert s.relax_torque(max_torque=0.05, check_every_nth_step=5, max_steps=20000)
+    assert s.last_relax_value < 0.05
+    assert s.stats["steps"] % 5 == 0
+    orc = oracle_mod.Solver(dims, delta, np.full(n, 1e6), A=np.full(n, 1.5e-11), alpha=np.full(n, 0.5),
+                            terms=("demag", "exchange"), tensor=oracle_mod.demag_tensor(*dims, *delta),
+                            float_norm=False)
+    orc.M = s.M.cpu().numpy()
+    assert orc.relax_norms()[2] == pytest.approx(s.last_relax_value, rel=1e-9)

@@ -16,9 +16,11 @@
 //    (SymmetricMatrixVectorConvolution_FFT.cpp:60-64 notes but does not use this);
 //  * for 2-D problems (nz == 1) the forward y FFT, the multiply and the inverse y FFT are one
 //    kernel.
-// Spectra layout: cplx<T> S[c][z][y][kx], c < 3, z < nz, y < py, kx < hx.
+// Spectra layout: cplx<T> S[c][z][y][kx], c < 3, z < nz, y < py, kx < hx, rows lx >= hx apart
+// (lx even in FP32, so that every row starts on a 16-byte boundary).
 #include "conv.cuh"
 #include "fft_reg.cuh"
+#include "tma.cuh"
 
 #include <cmath>
 #include <vector>
@@ -75,7 +77,7 @@ __device__ __forceinline__ void load_twiddles(cplx<T> *tw_s, const cplx<T> *tw_g
 template <typename T, bool SCALE>
 __global__ void __launch_bounds__(NT) k_x_fwd(const T *__restrict__ M, const uint8_t *__restrict__ reg,
                                              const T *__restrict__ ms_tab, cplx<T> *__restrict__ S,
-                                             int nx, int ny, int nz, int py, int hx, FftRadices rad,
+                                             int nx, int ny, int nz, int py, int hx, int lx, FftRadices rad,
                                              const cplx<T> *__restrict__ tw_g, int LP)
 {
 	using C = cplx<T>;
@@ -115,12 +117,12 @@ __global__ void __launch_bounds__(NT) k_x_fwd(const T *__restrict__ M, const uin
 		if (ra < rows) {
 			const int c = ra / nyz, rem = ra % nyz;
 			const size_t srow = (size_t)(c * nz + rem / ny) * py + rem % ny;
-			S[srow * hx + k] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
+			S[srow * lx + k] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
 		}
 		if (rb < rows) {
 			const int c = rb / nyz, rem = rb % nyz;
 			const size_t srow = (size_t)(c * nz + rem / ny) * py + rem % ny;
-			S[srow * hx + k] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
+			S[srow * lx + k] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
 		}
 	}
 }
@@ -128,7 +130,7 @@ __global__ void __launch_bounds__(NT) k_x_fwd(const T *__restrict__ M, const uin
 // ---- x inverse: half spectra -> real rows ------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(NT) k_x_inv(const cplx<T> *__restrict__ S, T *__restrict__ H,
-                                             int nx, int ny, int nz, int py, int hx, FftRadices rad,
+                                             int nx, int ny, int nz, int py, int hx, int lx, FftRadices rad,
                                              const cplx<T> *__restrict__ tw_g, int LP)
 {
 	using C = cplx<T>;
@@ -152,11 +154,11 @@ __global__ void __launch_bounds__(NT) k_x_inv(const cplx<T> *__restrict__ S, T *
 		C A = {0, 0}, B = {0, 0};
 		if (ra < rows) {
 			const int c = ra / nyz, rem = ra % nyz;
-			A = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * hx + kk];
+			A = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * lx + kk];
 		}
 		if (rb < rows) {
 			const int c = rb / nyz, rem = rb % nyz;
-			B = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * hx + kk];
+			B = S[((size_t)(c * nz + rem / ny) * py + rem % ny) * lx + kk];
 		}
 		if (realonly) { A.y = 0; B.y = 0; }
 		if (mirror) { A.y = -A.y; B.y = -B.y; }
@@ -176,7 +178,7 @@ __global__ void __launch_bounds__(NT) k_x_inv(const cplx<T> *__restrict__ S, T *
 // ---- y pass (3-D): column tiles, forward pads ny -> py, inverse crops py -> ny -----------------
 template <typename T, bool INV>
 __global__ void __launch_bounds__(NT) k_y(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
-                                         int py, int hx, FftRadices rad,
+                                         int py, int hx, int lx, FftRadices rad,
                                          const cplx<T> *__restrict__ tw_g, int TB)
 {
 	using C = cplx<T>;
@@ -187,16 +189,16 @@ __global__ void __launch_bounds__(NT) k_y(cplx<T> *__restrict__ S, int n_in, int
 	load_twiddles<T>(tw, tw_g, py);
 	const int kx0 = blockIdx.x * TB;
 	const int z = blockIdx.y, c = blockIdx.z;
-	C *base = S + (size_t)(c * nz + z) * py * hx;
+	C *base = S + (size_t)(c * nz + z) * py * lx;
 	for (int e = threadIdx.x; e < TB * py; e += blockDim.x) {
 		const int y = e / TB, b = e % TB;
-		b0[e] = (y < n_in && kx0 + b < hx) ? base[(size_t)y * hx + kx0 + b] : C{0, 0};
+		b0[e] = (y < n_in && kx0 + b < hx) ? base[(size_t)y * lx + kx0 + b] : C{0, 0};
 	}
 	__syncthreads();
 	C *res = fft_lines<T, INV>(b0, b1, 1, TB, TB, rad, tw);
 	for (int e = threadIdx.x; e < TB * n_out; e += blockDim.x) {
 		const int y = e / TB, b = e % TB;
-		if (kx0 + b < hx) base[(size_t)y * hx + kx0 + b] = res[e];
+		if (kx0 + b < hx) base[(size_t)y * lx + kx0 + b] = res[e];
 	}
 }
 
@@ -217,7 +219,7 @@ __device__ __forceinline__ void tensor_apply(const T *__restrict__ t, size_t cs,
 // ---- z pass (3-D): forward FFT along z, tensor multiply, inverse FFT, all three components ----
 template <typename T>
 __global__ void __launch_bounds__(NT) k_z_mul(cplx<T> *__restrict__ S, const T *__restrict__ Nt,
-                                             int nz, int py, int hx, int qy, int qz, FftRadices rad,
+                                             int nz, int py, int hx, int lx, int qy, int qz, FftRadices rad,
                                              const cplx<T> *__restrict__ tw_g, int TB)
 {
 	using C = cplx<T>;
@@ -230,10 +232,10 @@ __global__ void __launch_bounds__(NT) k_z_mul(cplx<T> *__restrict__ S, const T *
 	const int kx0 = blockIdx.x * TB;
 	const int ky = blockIdx.y;
 	const int L = 3 * TB;
-	const size_t cstride = (size_t)nz * py * hx;
+	const size_t cstride = (size_t)nz * py * lx;
 	for (int e = threadIdx.x; e < L * pz; e += blockDim.x) {
 		const int zz = e / L, l = e % L, c = l / TB, b = l % TB;
-		b0[e] = (zz < nz && kx0 + b < hx) ? S[c * cstride + ((size_t)zz * py + ky) * hx + kx0 + b] : C{0, 0};
+		b0[e] = (zz < nz && kx0 + b < hx) ? S[c * cstride + ((size_t)zz * py + ky) * lx + kx0 + b] : C{0, 0};
 	}
 	__syncthreads();
 	C *res = fft_lines<T, false>(b0, b1, 1, L, L, rad, tw);
@@ -256,14 +258,14 @@ __global__ void __launch_bounds__(NT) k_z_mul(cplx<T> *__restrict__ S, const T *
 	C *out = fft_lines<T, true>(res, other, 1, L, L, rad, tw);
 	for (int e = threadIdx.x; e < L * nz; e += blockDim.x) {
 		const int zz = e / L, l = e % L, c = l / TB, b = l % TB;
-		if (kx0 + b < hx) S[c * cstride + ((size_t)zz * py + ky) * hx + kx0 + b] = out[e];
+		if (kx0 + b < hx) S[c * cstride + ((size_t)zz * py + ky) * lx + kx0 + b] = out[e];
 	}
 }
 
 // ---- y pass with multiply (2-D problems): forward y FFT, tensor multiply, inverse y FFT -------
 template <typename T>
 __global__ void __launch_bounds__(NT) k_y_mul2d(cplx<T> *__restrict__ S, const T *__restrict__ Nt,
-                                               int ny, int hx, int qy, FftRadices rad,
+                                               int ny, int hx, int lx, int qy, FftRadices rad,
                                                const cplx<T> *__restrict__ tw_g, int TB)
 {
 	using C = cplx<T>;
@@ -275,10 +277,10 @@ __global__ void __launch_bounds__(NT) k_y_mul2d(cplx<T> *__restrict__ S, const T
 	load_twiddles<T>(tw, tw_g, py);
 	const int kx0 = blockIdx.x * TB;
 	const int L = 3 * TB;
-	const size_t cstride = (size_t)py * hx;
+	const size_t cstride = (size_t)py * lx;
 	for (int e = threadIdx.x; e < L * py; e += blockDim.x) {
 		const int y = e / L, l = e % L, c = l / TB, b = l % TB;
-		b0[e] = (y < ny && kx0 + b < hx) ? S[c * cstride + (size_t)y * hx + kx0 + b] : C{0, 0};
+		b0[e] = (y < ny && kx0 + b < hx) ? S[c * cstride + (size_t)y * lx + kx0 + b] : C{0, 0};
 	}
 	__syncthreads();
 	C *res = fft_lines<T, false>(b0, b1, 1, L, L, rad, tw);
@@ -298,7 +300,7 @@ __global__ void __launch_bounds__(NT) k_y_mul2d(cplx<T> *__restrict__ S, const T
 	C *out = fft_lines<T, true>(res, other, 1, L, L, rad, tw);
 	for (int e = threadIdx.x; e < L * ny; e += blockDim.x) {
 		const int y = e / L, l = e % L, c = l / TB, b = l % TB;
-		if (kx0 + b < hx) S[c * cstride + (size_t)y * hx + kx0 + b] = out[e];
+		if (kx0 + b < hx) S[c * cstride + (size_t)y * lx + kx0 + b] = out[e];
 	}
 }
 
@@ -407,7 +409,7 @@ __host__ __device__ constexpr int ct_lpb(int n, int csize)
 // y pass (3-D): TB columns per CTA; forward pads rows n_in -> N, inverse crops N -> n_out.
 template <typename T, int N, int TB, bool INV>
 __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
-                                                                 int hx, const cplx<T> *__restrict__ twN)
+                                                                 int hx, int lx, const cplx<T> *__restrict__ twN)
 {
 	using C = cplx<T>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -416,10 +418,10 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__r
 	const int line = tid & (TB - 1), j0 = tid / TB;
 	const int kx = blockIdx.x * TB + line;
 	const bool ok = kx < hx;
-	C *base = S + (size_t)(blockIdx.z * nz + blockIdx.y) * N * hx + (ok ? kx : 0);
-	auto ld = [&](int, int k) -> C { return (ok && k < n_in) ? base[(size_t)k * hx] : C{0, 0}; };
+	C *base = S + (size_t)(blockIdx.z * nz + blockIdx.y) * N * lx + (ok ? kx : 0);
+	auto ld = [&](int, int k) -> C { return (ok && k < n_in) ? base[(size_t)k * lx] : C{0, 0}; };
 	auto st = [&](int, int k, C v) {
-		if (ok && k < n_out) base[(size_t)k * hx] = v;
+		if (ok && k < n_out) base[(size_t)k * lx] = v;
 	};
 	cta_fft<T, N, ct_radix(N), TB, INV, SmCols<N, TB>>(sm, twN, line, j0, ld, st);
 }
@@ -430,7 +432,7 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
                                                                      const uint8_t *__restrict__ reg,
                                                                      const T *__restrict__ ms_tab,
                                                                      cplx<T> *__restrict__ S, int nx, int ny, int nz,
-                                                                     int py, int hx, const cplx<T> *__restrict__ twN)
+                                                                     int py, int hx, int lx, const cplx<T> *__restrict__ twN)
 {
 	using C = cplx<T>;
 	constexpr int TPL = N / ct_radix(N);
@@ -457,8 +459,8 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
 	auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
 	cta_fft<T, N, ct_radix(N), LPB, false, SI>(sm, twN, line, j0, ld, st);
 	__syncthreads();
-	C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * hx;
-	C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * hx;
+	C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
+	C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
 	const T h = T(0.5);
 	for (int k = j0; k < hx; k += TPL) {
 		const C zk = sm[SI::at(line, k)], zn = sm[SI::at(line, (N - k) & (N - 1))];
@@ -470,7 +472,7 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
 // x pass inverse: half spectra of rows 2q, 2q+1 -> real rows.
 template <typename T, int N, int LPB>
 __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx<T> *__restrict__ S, T *__restrict__ H,
-                                                                     int nx, int ny, int nz, int py, int hx,
+                                                                     int nx, int ny, int nz, int py, int hx, int lx,
                                                                      const cplx<T> *__restrict__ twN)
 {
 	using C = cplx<T>;
@@ -484,8 +486,8 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx
 	const int ra = 2 * (blockIdx.x * LPB + line), rb = ra + 1;
 	const bool va = ra < rows, vb = rb < rows;
 	const int qa = va ? ra : 0, qb = vb ? rb : 0;
-	const C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * hx;
-	const C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * hx;
+	const C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
+	const C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
 	T *Ha = H + (size_t)qa * nx, *Hb = H + (size_t)qb * nx;
 	auto ld = [&](int, int f) -> C {
 		const bool mirror = f >= hx;
@@ -511,7 +513,7 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx
 template <typename T, int PZ, int TB>
 __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> *__restrict__ S,
                                                                         const T *__restrict__ Nt, int nz, int py,
-                                                                        int hx, int qy, int qz,
+                                                                        int hx, int lx, int qy, int qz,
                                                                         const cplx<T> *__restrict__ twN)
 {
 	using C = cplx<T>;
@@ -524,11 +526,11 @@ __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> 
 	const int line = tid % LANES, j0 = tid / LANES;
 	const int c = line / TB, b = line % TB;
 	const int ky = blockIdx.y;
-	const size_t cstride = (size_t)nz * py * hx, zstride = (size_t)py * hx;
+	const size_t cstride = (size_t)nz * py * lx, zstride = (size_t)py * lx;
 	{
 		const int kx = blockIdx.x * TB + b;
 		const bool ok = kx < hx;
-		C *col = S + c * cstride + (size_t)ky * hx + (ok ? kx : 0);
+		C *col = S + c * cstride + (size_t)ky * lx + (ok ? kx : 0);
 		auto ld = [&](int, int z) -> C { return (ok && z < nz) ? col[z * zstride] : C{0, 0}; };
 		auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
 		cta_fft<T, PZ, R, LANES, false, SI>(sm, twN, line, j0, ld, st);
@@ -552,7 +554,7 @@ __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> 
 	{
 		const int kx = blockIdx.x * TB + b;
 		const bool ok = kx < hx;
-		C *col = S + c * cstride + (size_t)ky * hx + (ok ? kx : 0);
+		C *col = S + c * cstride + (size_t)ky * lx + (ok ? kx : 0);
 		auto ld = [&](int l, int k) -> C { return sm[SI::at(l, k)]; };
 		auto st = [&](int, int z, C v) {
 			if (ok && z < nz) col[z * zstride] = v;
@@ -573,7 +575,7 @@ constexpr int ZR_THREADS = 192;  // 32 kx x 3 components x 2 rows
 
 template <typename T, int PZ>
 __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
-                                                        int py, int hx, int qy, int qz)
+                                                        int py, int hx, int lx, int qy, int qz)
 {
 	using C = cplx<T>;
 	constexpr int H = PZ / 2;
@@ -585,8 +587,8 @@ __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S
 	const bool two = b > 0 && b1 != b;
 	const int kx = blockIdx.x * 32 + lane;
 	const bool ok = (r == 0 || two) && kx < hx;
-	const size_t zstride = (size_t)py * hx;
-	C *col = S + ((size_t)c * nz * py + (size_t)(r == 0 ? b : b1)) * hx + kx;
+	const size_t zstride = (size_t)py * lx;
+	C *col = S + ((size_t)c * nz * py + (size_t)(r == 0 ? b : b1)) * lx + kx;
 	C v[PZ];
 #pragma unroll
 	for (int z = 0; z < H; ++z) v[z] = (ok && z < nz) ? col[z * zstride] : C{0, 0};
@@ -632,7 +634,90 @@ void fs_z_reg(ConvPlan *p, cudaStream_t st)
 {
 	const dim3 grid((p->hx + 31) / 32, p->qy);
 	k_z_reg<T, PZ><<<grid, ZR_THREADS, (size_t)2 * PZ * 96 * sizeof(cplx<T>), st>>>(
-	    (cplx<T> *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz);
+	    (cplx<T> *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->lx, p->qy, p->qz);
+}
+
+// ---- y pass through TMA-staged tiles -------------------------------------------------------------
+// Persistent CTAs walk tiles (TB columns of one (component, z) plane).  Each tile's input rows
+// (the ny < N/2 data rows padded to N/2 by the TMA unit's zero fill going forward, all N rows
+// going back) arrive by cp.async.bulk.tensor in one of two stage buffers while the previous tile is
+// transformed; pass 0 reads the stage buffer, the later passes work in a skewed shared-memory
+// buffer, and the last pass stores straight to HBM.  Thread 0 issues the loads; a bounded wait that
+// runs out sets *err and ends the kernel instead of hanging.
+template <int N, int TB, bool INV, class C>
+struct YTmaGeom {
+	static constexpr int ROWS = INV ? N : N / 2;
+	static constexpr int BR = ROWS < 256 ? ROWS : 256;
+	static constexpr int NBOX = ROWS / BR;
+	static constexpr int E = (int)(sizeof(C) / 8);
+	static constexpr uint32_t TILE_BYTES = (uint32_t)(TB * ROWS * sizeof(C));
+	static constexpr size_t WORK = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 15) / 16 * 16;
+	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
+};
+
+template <typename T, int N, int TB, bool INV>
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 1)
+    k_y_tma(const __grid_constant__ CUtensorMap tmap, cplx<T> *__restrict__ S, int n_out, int hx, int lx,
+            int tiles_x, int ntiles, const cplx<T> *__restrict__ twN, int *err)
+{
+	using C = cplx<T>;
+	using G = YTmaGeom<N, TB, INV, C>;
+	constexpr int R = ct_radix(N);
+	using SI = SmCols<N, TB>;
+	extern __shared__ __align__(128) unsigned char smem_tma[];
+	C *stage0 = reinterpret_cast<C *>(smem_tma);
+	C *stage1 = stage0 + TB * G::ROWS;
+	C *work = reinterpret_cast<C *>(smem_tma + 2 * (size_t)G::TILE_BYTES);
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * (size_t)G::TILE_BYTES + G::WORK);
+	const int tid = threadIdx.x;
+	const int line = tid & (TB - 1), j0 = tid / TB;
+	auto issue = [&](int t, int b) {
+		const int tx = t % tiles_x, plane = t / tiles_x;
+		C *dst = b ? stage1 : stage0;
+		mbar_expect_tx(&bar[b], G::TILE_BYTES);
+#pragma unroll
+		for (int q = 0; q < G::NBOX; ++q)
+			tma_load_3d(dst + q * G::BR * TB, &tmap, tx * TB * G::E, q * G::BR, plane, &bar[b]);
+	};
+	if (tid == 0) {
+		mbar_init(&bar[0], 1);
+		mbar_init(&bar[1], 1);
+		fence_proxy_async();
+	}
+	__syncthreads();
+	if (tid == 0) {
+		if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+		if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
+	}
+	uint32_t parity = 0;  // bit b: phase parity expected next on bar[b]
+	int k = 0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+		const int b = k & 1;
+		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+		if (__syncthreads_or(late)) {
+			if (tid == 0) atomicExch(err, 1);
+			return;
+		}
+		parity ^= 1u << b;
+		const int tx = t % tiles_x, plane = t / tiles_x;
+		const int kx = tx * TB + line;
+		const bool ok = kx < hx;
+		C *base = S + (size_t)plane * N * lx + (ok ? kx : 0);
+		const C *sb = b ? stage1 : stage0;
+		auto ld = [&](int, int r) -> C { return r < G::ROWS ? sb[r * TB + line] : C{0, 0}; };
+		auto st = [&](int, int r, C v) {
+			if (ok && r < n_out) base[(size_t)r * lx] = v;
+		};
+		const int next = t + 2 * (int)gridDim.x;
+		auto release = [&]() {
+			__syncthreads();  // every thread has read stage buffer b
+			if (tid == 0 && next < ntiles) {
+				fence_proxy_async();
+				issue(next, b);
+			}
+		};
+		cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
+	}
 }
 
 // ---- fast-path geometry and dispatch ---------------------------------------------------------------
@@ -659,6 +744,51 @@ mm_status fs_setup_len()
 	return MM_OK;
 }
 
+// TMA-staged y passes: tensor maps over the spectrum, shared-memory size, persistent grid size.
+// Used when the inverse pass's stage buffers fit in shared memory and the forward input is at
+// most half the padded length (ny <= py/2, the zero padding the first pass relies on).
+template <typename T, int N>
+mm_status fs_setup_y_tma(ConvPlan *p)
+{
+	using C = cplx<T>;
+	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	using GF = YTmaGeom<N, TB, false, C>;
+	using GI = YTmaGeom<N, TB, true, C>;
+	p->tma_y = false;
+	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || TB * sizeof(C) < 16) return MM_OK;
+	constexpr int E = GF::E;
+	const uint64_t d0 = (uint64_t)p->lx * E, rowb = (uint64_t)p->lx * sizeof(C), planeb = rowb * p->py;
+	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, TB * E, GF::BR, 1));
+	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, TB * E, GI::BR, 1));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, false>, GF::SMEM));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, true>, GI::SMEM));
+	int bf = 0, bi = 0;
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, TB, false>, THREADS, GF::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, TB, true>, THREADS, GI::SMEM));
+	if (bf < 1 || bi < 1) return MM_OK;
+	p->grid_yf = bf * num_sms();
+	p->grid_yi = bi * num_sms();
+	if (!p->err) {
+		MM_CUDA(cudaMalloc(&p->err, sizeof(int)));
+		MM_CUDA(cudaMemset(p->err, 0, sizeof(int)));
+	}
+	p->tma_y = true;
+	return MM_OK;
+}
+
+template <typename T, int N, bool INV>
+void fs_y_tma(ConvPlan *p, cudaStream_t st)
+{
+	using C = cplx<T>;
+	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	using G = YTmaGeom<N, TB, INV, C>;
+	const int tiles_x = (p->hx + TB - 1) / TB, ntiles = tiles_x * 3 * p->nz;
+	const int grid = std::min(ntiles, INV ? p->grid_yi : p->grid_yf);
+	k_y_tma<T, N, TB, INV><<<grid, THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
+	                                                       INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
+	                                                       (const C *)p->tw_y, p->err);
+}
+
 template <typename T, int N>
 void fs_x_fwd(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, cudaStream_t st)
 {
@@ -669,10 +799,10 @@ void fs_x_fwd(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, cuda
 	const size_t smem = (size_t)SmRows<N, LPB>::SIZE * sizeof(C);
 	if (ms_tab)
 		k_x_fwd_ct<T, N, LPB, true><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
-		                                                       p->py, p->hx, (const C *)p->tw_x);
+		                                                       p->py, p->hx, p->lx, (const C *)p->tw_x);
 	else
 		k_x_fwd_ct<T, N, LPB, false><<<grid, block, smem, st>>>(M, reg, ms_tab, (C *)p->spec, p->nx, p->ny, p->nz,
-		                                                        p->py, p->hx, (const C *)p->tw_x);
+		                                                        p->py, p->hx, p->lx, (const C *)p->tw_x);
 }
 
 template <typename T, int N>
@@ -683,7 +813,7 @@ void fs_x_inv(ConvPlan *p, T *H, cudaStream_t st)
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
 	const dim3 grid((lines + LPB - 1) / LPB), block(LPB * TPL);
 	k_x_inv_ct<T, N, LPB><<<grid, block, (size_t)SmRows<N, LPB>::SIZE * sizeof(C), st>>>(
-	    (const C *)p->spec, H, p->nx, p->ny, p->nz, p->py, p->hx, (const C *)p->tw_x);
+	    (const C *)p->spec, H, p->nx, p->ny, p->nz, p->py, p->hx, p->lx, (const C *)p->tw_x);
 }
 
 template <typename T, int N, bool INV>
@@ -693,7 +823,7 @@ void fs_y(ConvPlan *p, cudaStream_t st)
 	constexpr int TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
 	const dim3 grid((p->hx + TB - 1) / TB, p->nz, 3), block(TB * TPL);
 	k_y_ct<T, N, TB, INV><<<grid, block, (size_t)SmCols<N, TB>::SIZE * sizeof(C), st>>>(
-	    (C *)p->spec, INV ? N : p->ny, INV ? p->ny : N, p->nz, p->hx, (const C *)p->tw_y);
+	    (C *)p->spec, INV ? N : p->ny, INV ? p->ny : N, p->nz, p->hx, p->lx, (const C *)p->tw_y);
 }
 
 constexpr int CT_ZTB = 32;
@@ -704,7 +834,7 @@ void fs_z(ConvPlan *p, cudaStream_t st)
 	using C = cplx<T>;
 	const dim3 grid((p->hx + CT_ZTB - 1) / CT_ZTB, p->py), block(3 * CT_ZTB * (PZ / ct_radix8(PZ)));
 	k_z_ct<T, PZ, CT_ZTB><<<grid, block, (size_t)SmCols<PZ, 3 * CT_ZTB>::SIZE * sizeof(C), st>>>(
-	    (C *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz, (const C *)p->tw_z);
+	    (C *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->lx, p->qy, p->qz, (const C *)p->tw_z);
 }
 
 #define MM_FS_SWITCH(n, CALL)                                                                    \
@@ -734,6 +864,9 @@ mm_status fs_setup(ConvPlan *p)
 	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_SETUP); MM_TRY(r); }
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_SETUP); MM_TRY(r); }
 #undef MM_SETUP
+#define MM_YTSETUP(N) r = fs_setup_y_tma<T, N>(p)
+	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_YTSETUP); MM_TRY(r); }
+#undef MM_YTSETUP
 	p->reg_z = p->fast_z && 2 * p->nz <= p->pz && p->pz <= (sizeof(T) == 4 ? 32 : 16);
 	if (p->reg_z) {
 		const size_t sz = (size_t)2 * p->pz * 96 * sizeof(cplx<T>);
@@ -877,29 +1010,33 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		MM_FS_SWITCH(p->px, MM_XF);
 #undef MM_XF
 	} else if (ms_tab)
-		k_x_fwd<T, true><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
+		k_x_fwd<T, true><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx, p->lx,
 		                                            p->rx, (const C *)p->tw_x, p->lp_x);
 	else
-		k_x_fwd<T, false><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx,
+		k_x_fwd<T, false><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx, p->lx,
 		                                             p->rx, (const C *)p->tw_x, p->lp_x);
 	MM_TRY(after_launch("k_x_fwd"));
 	prof_end(tk, "k_x_fwd", 3 * n * s + (reg ? n : 0.0) + half, st);
 	if (p->is2d) {
 		const int gy = (p->hx + p->tb_y - 1) / p->tb_y;
 		tk = prof_begin(st);
-		k_y_mul2d<T><<<gy, NT, p->smem_y, st>>>(S, (const T *)p->tensor, p->ny, p->hx, p->qy, p->ry,
+		k_y_mul2d<T><<<gy, NT, p->smem_y, st>>>(S, (const T *)p->tensor, p->ny, p->hx, p->lx, p->qy, p->ry,
 		                                        (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_mul2d"));
 		prof_end(tk, "k_y_mul2d", 2 * half + tens, st);
 	} else {
 		dim3 gy((p->hx + p->tb_y - 1) / p->tb_y, p->nz, 3);
 		tk = prof_begin(st);
-		if (p->fast_y) {
+		if (p->tma_y) {
+#define MM_YTF(N) fs_y_tma<T, N, false>(p, st)
+			MM_FS_SWITCH(p->py, MM_YTF);
+#undef MM_YTF
+		} else if (p->fast_y) {
 #define MM_YF(N) fs_y<T, N, false>(p, st)
 			MM_FS_SWITCH(p->py, MM_YF);
 #undef MM_YF
 		} else
-			k_y<T, false><<<gy, NT, p->smem_y, st>>>(S, p->ny, p->py, p->nz, p->py, p->hx, p->ry,
+			k_y<T, false><<<gy, NT, p->smem_y, st>>>(S, p->ny, p->py, p->nz, p->py, p->hx, p->lx, p->ry,
 			                                         (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_fwd"));
 		prof_end(tk, "k_y_fwd", half + ypad, st);
@@ -923,17 +1060,21 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 			case 64: fs_z<T, 64>(p, st); break;
 			}
 		} else
-			k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->qy, p->qz,
+			k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->lx, p->qy, p->qz,
 			                                      p->rz, (const C *)p->tw_z, p->tb_z);
 		MM_TRY(after_launch("k_z_mul"));
 		prof_end(tk, "k_z_mul", 2 * ypad + tens, st);
 		tk = prof_begin(st);
-		if (p->fast_y) {
+		if (p->tma_y) {
+#define MM_YTI(N) fs_y_tma<T, N, true>(p, st)
+			MM_FS_SWITCH(p->py, MM_YTI);
+#undef MM_YTI
+		} else if (p->fast_y) {
 #define MM_YI(N) fs_y<T, N, true>(p, st)
 			MM_FS_SWITCH(p->py, MM_YI);
 #undef MM_YI
 		} else
-			k_y<T, true><<<gy, NT, p->smem_y, st>>>(S, p->py, p->ny, p->nz, p->py, p->hx, p->ry,
+			k_y<T, true><<<gy, NT, p->smem_y, st>>>(S, p->py, p->ny, p->nz, p->py, p->hx, p->lx, p->ry,
 			                                        (const C *)p->tw_y, p->tb_y);
 		MM_TRY(after_launch("k_y_inv"));
 		prof_end(tk, "k_y_inv", half + ypad, st);
@@ -944,7 +1085,7 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		MM_FS_SWITCH(p->px, MM_XI);
 #undef MM_XI
 	} else
-		k_x_inv<T><<<gx, NT, p->smem_x, st>>>(S, H, p->nx, p->ny, p->nz, p->py, p->hx, p->rx,
+		k_x_inv<T><<<gx, NT, p->smem_x, st>>>(S, H, p->nx, p->ny, p->nz, p->py, p->hx, p->lx, p->rx,
 		                                      (const C *)p->tw_x, p->lp_x);
 	MM_TRY(after_launch("k_x_inv"));
 	prof_end(tk, "k_x_inv", half + 3 * n * s, st);
@@ -970,7 +1111,38 @@ mm_status fft_reg_init()
 size_t ConvPlan::spec_bytes() const
 {
 	const size_t c = prec == MM_F64 ? sizeof(double2) : sizeof(float2);
-	return c * 3 * (size_t)nz * py * hx;
+	return c * 3 * (size_t)nz * py * lx;
+}
+
+mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                        uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2)
+{
+	using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+	                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+	                            CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+	static Encode encode = nullptr;
+	if (!encode) {
+		void *fn = nullptr;
+		cudaDriverEntryPointQueryResult q{};
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+		    q != cudaDriverEntryPointSuccess || !fn) {
+			cudaGetLastError();
+			return fail(MM_ERR_UNSUPPORTED, "conv: cuTensorMapEncodeTiled is not available from the driver");
+		}
+		encode = reinterpret_cast<Encode>(fn);
+	}
+	if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride1 & 15) || (stride2 & 15) || ((b0 * 8) & 15))
+		return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map not 16-byte aligned");
+	const cuuint64_t dims[3] = {d0, d1, d2};
+	const cuuint64_t strides[2] = {stride1, stride2};
+	const cuuint32_t box[3] = {b0, b1, b2};
+	const cuuint32_t estr[3] = {1, 1, 1};
+	const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(base), dims, strides, box,
+	                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+	                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if (r != CUDA_SUCCESS)
+		return fail(MM_ERR_CUDA, "conv: cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+	return MM_OK;
 }
 
 ConvPlan::~ConvPlan()
@@ -980,6 +1152,7 @@ ConvPlan::~ConvPlan()
 	cudaFree(tw_z);
 	cudaFree(tensor);
 	cudaFree(spec);
+	cudaFree(err);
 }
 
 int conv_launches(const ConvPlan *p) { return p->is2d ? 3 : 5; }
@@ -995,6 +1168,7 @@ mm_status conv_plan_create(ConvPlan **out, int prec, int nx, int ny, int nz, int
 	p->nx = nx; p->ny = ny; p->nz = nz;
 	p->px = px; p->py = py; p->pz = pz;
 	p->hx = px / 2 + 1;
+	p->lx = (prec == MM_F32) ? (p->hx + 1) & ~1 : p->hx;
 	p->qy = py / 2 + 1;
 	p->qz = pz / 2 + 1;
 	p->is2d = (nz == 1 && pz == 1);

@@ -1,6 +1,8 @@
 // Zero-padded FFT convolution H = N * M with the symmetric demag tensor (internal API).
 #pragma once
 
+#include <cuda.h>
+
 #include "mm_common.cuh"
 #include "fft.cuh"
 
@@ -11,14 +13,19 @@ struct ConvPlan {
 	int nx = 0, ny = 0, nz = 0;     // grid
 	int px = 0, py = 0, pz = 0;     // padded (FFT) lengths
 	int hx = 0;                     // px/2 + 1 stored x frequencies
+	int lx = 0;                     // spectrum row stride (hx, rounded up to even in FP32: 16-byte rows)
 	int qy = 0, qz = 0;             // py/2 + 1, pz/2 + 1 stored tensor frequencies
 	bool is2d = false;              // nz == 1 && pz == 1
 	bool fast_x = false, fast_y = false, fast_z = false;  // power-of-two register-FFT passes
 	bool reg_z = false;             // z pass with whole columns in registers (nz <= pz/2, pz small)
+	bool tma_y = false;             // y passes fed by TMA-staged tiles (persistent CTAs)
+	CUtensorMap tm_yf{}, tm_yi{};   // spectrum views of the forward (ny rows) and inverse (py rows) y pass
+	int grid_yf = 0, grid_yi = 0;   // persistent grid sizes of those passes
+	int *err = nullptr;             // device word set when a bounded wait of a staged pass gave up
 	FftRadices rx{}, ry{}, rz{};
 	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
 	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]
-	void *spec = nullptr;           // cplx<T>[3][nz][py][hx]
+	void *spec = nullptr;           // cplx<T>[3][nz][py][lx]
 	// launch geometry
 	int lp_x = 1;                   // complex lines (= 2 real rows) per CTA in the x passes
 	int tb_y = 1, tb_z = 1;         // columns per CTA in the y and z passes

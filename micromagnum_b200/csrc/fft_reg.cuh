@@ -121,9 +121,16 @@ struct SmRows {  // element (line, k) at line * N + k
 	__device__ __forceinline__ static int at(int line, int k) { return sm_pad(line * N + k); }
 };
 
-template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, class LD, class ST>
+// Hook run by every thread after pass 0 has stored its outputs (a no-op unless a kernel stages
+// its inputs and can release their buffer once pass 0 has read them).
+struct NoHook {
+	__device__ __forceinline__ void operator()() const {}
+};
+
+template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, class LD, class ST,
+          class HK = NoHook>
 __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0,
-                                             LD &ld, ST &st)
+                                             LD &ld, ST &st, HK hk = HK())
 {
 	using C = cplx<T>;
 	constexpr int P = fft_npasses(N, R);
@@ -167,16 +174,18 @@ __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restr
 			else sm[SmIdx::at(line, base + k * Ns)] = val;
 		}
 	}
-	if constexpr (p + 1 < P) cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, p + 1>(sm, twN, line, j0, ld, st);
+	if constexpr (p == 0) hk();
+	if constexpr (p + 1 < P) cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, p + 1>(sm, twN, line, j0, ld, st, hk);
 }
 
 // LD_SM: the loader reads the same shared memory the passes write (adds a barrier after pass 0's
 // reads).
-template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM = false, class LD, class ST>
+template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM = false, class LD, class ST,
+          class HK = NoHook>
 __device__ __forceinline__ void cta_fft(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0, LD &ld,
-                                        ST &st)
+                                        ST &st, HK hk = HK())
 {
-	cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, 0>(sm, twN, line, j0, ld, st);
+	cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, 0>(sm, twN, line, j0, ld, st, hk);
 }
 
 } // namespace mm

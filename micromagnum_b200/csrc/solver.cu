@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(256) k_accept(size_t n, const T *__restrict__ 
 // 35-73), in double, on one thread; also swaps k_0 / k_last for first-same-as-last tableaus.
 template <typename T>
 __global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double eps_rel, int order,
-                             int fsal, int s, DevState *host_copy)
+                             int fsal, int s, DevState *host_copy, const int *conv_timeout)
 {
 	const double h = st->h;
 	const double e_abs = sqrt(st->max_err2);
@@ -423,10 +423,11 @@ __global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double
 		h_new = fmin(fmax(h * sc, 1e-15), 1e-10);
 		if (h_new == 1e-15) accept = 1;
 	}
-	if (!finite) accept = 0;
+	const int timed_out = conv_timeout ? *conv_timeout : 0;
+	if (!finite || timed_out) accept = 0;
 	st->accept = accept;
 	st->h_new = h_new;
-	st->not_finite = !finite;
+	st->not_finite = timed_out ? 2 : !finite;
 	*host_copy = *st;
 	st->max_err2 = 0.0;
 	st->max_k02 = 0.0;
@@ -711,6 +712,9 @@ dim3 stage_grid(const mm_solver_config &c)
 	return dim3((c.nx + 32 * STAGE_CPT - 1) / (32 * STAGE_CPT), (c.ny + 7) / 8, c.nz);
 }
 
+// Device word a staged convolution pass sets when a bounded wait gave up (NULL without one).
+const int *conv_timeout_flag(const mm_solver *s) { return s->conv ? s->conv->err : nullptr; }
+
 // Demag field of the state y (unit, T) into s->hd.
 template <typename T>
 mm_status demag(mm_solver *s, const void *y, cudaStream_t st)
@@ -867,7 +871,7 @@ template <typename T>
 mm_status controller(mm_solver *s, cudaStream_t st)
 {
 	k_controller<T><<<1, 1, 0, st>>>(s->dst, (KTab<T> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel, s->tab.order,
-	                                 s->tab.fsal, s->tab.s, s->hst);
+	                                 s->tab.fsal, s->tab.s, s->hst, conv_timeout_flag(s));
 	MM_TRY(after_launch("k_controller"));
 	MM_CUDA(cudaStreamSynchronize(st));
 	return MM_OK;
@@ -920,7 +924,7 @@ mm_status attempt_graph(mm_solver *s, bool eval_k0, cudaStream_t st)
 		if (r == MM_OK) r = attempt<T>(s, eval_k0, st);
 		if (r == MM_OK) {
 			k_controller<T><<<1, 1, 0, st>>>(s->dst, (KTab<T> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
-			                                 s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+			                                 s->tab.order, s->tab.fsal, s->tab.s, s->hst, conv_timeout_flag(s));
 			r = after_launch("k_controller");
 		}
 		cudaGraph_t g = nullptr;
@@ -975,6 +979,8 @@ mm_status evolve(mm_solver *s, double t_max, cudaStream_t st)
 	for (;;) {
 		MM_TRY(attempt_and_control<T>(s, h_try, st));
 		const DevState &d = *s->hst;
+		if (d.not_finite == 2)
+			return fail(MM_ERR_TIMEOUT, "solver: a TMA-staged FFT pass gave up waiting for its loads");
 		if (d.not_finite) {
 			s->not_finite = 1;
 			return fail(MM_ERR_NOT_FINITE, "solver: non-finite value in the state or its derivative");
@@ -1255,11 +1261,11 @@ MM_API mm_status mm_solver_attempt(mm_solver *s, double h, void *stream)
 	if (s->cfg.precision == MM_F64) {
 		MM_TRY(attempt<double>(s, eval_k0, st));
 		k_controller<double><<<1, 1, 0, st>>>(s->dst, (KTab<double> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
-		                                      s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+		                                      s->tab.order, s->tab.fsal, s->tab.s, s->hst, conv_timeout_flag(s));
 	} else {
 		MM_TRY(attempt<float>(s, eval_k0, st));
 		k_controller<float><<<1, 1, 0, st>>>(s->dst, (KTab<float> *)s->ktab, s->cfg.eps_abs, s->cfg.eps_rel,
-		                                     s->tab.order, s->tab.fsal, s->tab.s, s->hst);
+		                                     s->tab.order, s->tab.fsal, s->tab.s, s->hst, conv_timeout_flag(s));
 	}
 	MM_TRY(after_launch("k_controller"));
 	if (s->tab.fsal) s->k0_valid = true;

@@ -1,0 +1,76 @@
+// Tensor-memory-accelerator (TMA) staging helpers for the FFT passes: tensor-map encoding on the
+// host (through the runtime's driver entry point, so the library does not link libcuda), and the
+// mbarrier / cp.async.bulk.tensor primitives in inline PTX.  Loads only, never with cluster
+// multicast: every copy lands in the issuing CTA's own shared memory.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "mm_common.cuh"
+
+namespace mm {
+
+// 3-D tiled tensor map over an array of 8-byte elements: dims[0] fastest, strides in bytes of
+// dims 1 and 2 (multiples of 16), box[] elements per dimension (box[0] * 8 a multiple of 16).
+// Out-of-range elements of a box read as zero.
+mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                        uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2);
+
+// Spin limit of a bounded mbarrier wait (each try_wait already blocks for a while in hardware);
+// a wait that exceeds it reports a timeout instead of hanging the GPU.
+constexpr uint32_t TMA_WAIT_LIMIT = 1u << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+	return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// Makes barrier initialisation and earlier generic-proxy shared-memory accesses visible to the
+// async proxy (the TMA unit).
+__device__ __forceinline__ void fence_proxy_async()
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+	             : "memory");
+}
+
+// Bounded wait for the phase with the given parity to complete; false on timeout.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+	const uint32_t a = smem_u32(bar);
+	for (uint32_t it = 0; it < TMA_WAIT_LIMIT; ++it) {
+		uint32_t done = 0;
+		asm volatile(
+		    "{\n\t.reg .pred p;\n\t"
+		    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+		    "selp.u32 %0, 1, 0, p;\n\t}"
+		    : "=r"(done)
+		    : "r"(a), "r"(parity)
+		    : "memory");
+		if (done) return true;
+	}
+	return false;
+}
+
+// 3-D tiled load of one box into shared memory, completing on `bar` (transaction bytes).
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, uint64_t *bar)
+{
+	asm volatile(
+	    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+	    "[%5];" ::"r"(smem_u32(dst)),
+	    "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+	    : "memory");
+}
+
+} // namespace mm

@@ -638,42 +638,49 @@ void fs_z_reg(ConvPlan *p, cudaStream_t st)
 }
 
 // ---- y pass through TMA-staged tiles -------------------------------------------------------------
-// Persistent CTAs walk tiles (TB columns of one (component, z) plane).  Each tile's input rows
-// (the ny < N/2 data rows padded to N/2 by the TMA unit's zero fill going forward, all N rows
-// going back) arrive by cp.async.bulk.tensor in one of two stage buffers while the previous tile is
-// transformed; pass 0 reads the stage buffer, the later passes work in a skewed shared-memory
-// buffer, and the last pass stores straight to HBM.  Thread 0 issues the loads; a bounded wait that
-// runs out sets *err and ends the kernel instead of hanging.
-template <int N, int TB, bool INV, class C>
+// Persistent CTAs walk tiles (TB columns of one (component, z) plane).  A tile's input rows (the
+// ny <= N/2 data rows, padded to N/2 by the TMA unit's zero fill, going forward; all N rows going
+// back) arrive by cp.async.bulk.tensor in one of two buffers while the CTA transforms the previous
+// tile in the other.  The transform runs in place: pass 0 reads the row-major TMA layout and,
+// after a barrier, writes the skewed column layout that the later passes use; the last pass stores
+// straight to HBM, and the buffer is handed back to the TMA unit for the tile after next.  TB
+// columns make 32-byte rows (at least 256 threads for short transforms), so that three CTAs of
+// 256 threads share an SM.  Thread 0 issues the loads; a bounded wait that runs out sets *err and
+// ends the kernel instead of hanging.
+template <int N, bool INV, class C>
 struct YTmaGeom {
+	static constexpr int R = ct_radix(N);
+	static constexpr int TB0 = 32 / (int)sizeof(C), TBT = 256 / (N / R > 0 ? N / R : 1);
+	static constexpr int TB = TB0 > TBT ? TB0 : TBT;
+	static constexpr int THREADS = TB * (N / R);
 	static constexpr int ROWS = INV ? N : N / 2;
 	static constexpr int BR = ROWS < 256 ? ROWS : 256;
 	static constexpr int NBOX = ROWS / BR;
 	static constexpr int E = (int)(sizeof(C) / 8);
 	static constexpr uint32_t TILE_BYTES = (uint32_t)(TB * ROWS * sizeof(C));
-	static constexpr size_t WORK = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 15) / 16 * 16;
-	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
+	static constexpr size_t BUF = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 127) / 128 * 128;
+	static constexpr size_t SMEM = 2 * BUF + 16;
+	static constexpr int MINB = (3 * SMEM <= 227 * 1024 && THREADS <= 256) ? 3 : (2 * SMEM <= 227 * 1024 ? 2 : 1);
 };
 
-template <typename T, int N, int TB, bool INV>
-__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 1)
+template <typename T, int N, bool INV>
+__global__ void __launch_bounds__(YTmaGeom<N, INV, cplx<T>>::THREADS, YTmaGeom<N, INV, cplx<T>>::MINB)
     k_y_tma(const __grid_constant__ CUtensorMap tmap, cplx<T> *__restrict__ S, int n_out, int hx, int lx,
             int tiles_x, int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
 	using C = cplx<T>;
-	using G = YTmaGeom<N, TB, INV, C>;
-	constexpr int R = ct_radix(N);
+	using G = YTmaGeom<N, INV, C>;
+	constexpr int TB = G::TB;
 	using SI = SmCols<N, TB>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
-	C *stage0 = reinterpret_cast<C *>(smem_tma);
-	C *stage1 = stage0 + TB * G::ROWS;
-	C *work = reinterpret_cast<C *>(smem_tma + 2 * (size_t)G::TILE_BYTES);
-	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * (size_t)G::TILE_BYTES + G::WORK);
+	C *buf0 = reinterpret_cast<C *>(smem_tma);
+	C *buf1 = reinterpret_cast<C *>(smem_tma + G::BUF);
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
 	const int tid = threadIdx.x;
 	const int line = tid & (TB - 1), j0 = tid / TB;
 	auto issue = [&](int t, int b) {
 		const int tx = t % tiles_x, plane = t / tiles_x;
-		C *dst = b ? stage1 : stage0;
+		C *dst = b ? buf1 : buf0;
 		mbar_expect_tx(&bar[b], G::TILE_BYTES);
 #pragma unroll
 		for (int q = 0; q < G::NBOX; ++q)
@@ -703,20 +710,18 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 1)
 		const int kx = tx * TB + line;
 		const bool ok = kx < hx;
 		C *base = S + (size_t)plane * N * lx + (ok ? kx : 0);
-		const C *sb = b ? stage1 : stage0;
+		C *sb = b ? buf1 : buf0;
 		auto ld = [&](int, int r) -> C { return r < G::ROWS ? sb[r * TB + line] : C{0, 0}; };
 		auto st = [&](int, int r, C v) {
 			if (ok && r < n_out) base[(size_t)r * lx] = v;
 		};
+		cta_fft<T, N, G::R, TB, INV, SI, true>(sb, twN, line, j0, ld, st);
+		// hand the buffer back: every thread's generic accesses to it are ordered before the
+		// asynchronous copy that refills it
 		const int next = t + 2 * (int)gridDim.x;
-		auto release = [&]() {
-			__syncthreads();  // every thread has read stage buffer b
-			if (tid == 0 && next < ntiles) {
-				fence_proxy_async();
-				issue(next, b);
-			}
-		};
-		cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
+		fence_proxy_async();
+		__syncthreads();
+		if (tid == 0 && next < ntiles) issue(next, b);
 	}
 }
 
@@ -745,26 +750,25 @@ mm_status fs_setup_len()
 }
 
 // TMA-staged y passes: tensor maps over the spectrum, shared-memory size, persistent grid size.
-// Used when the inverse pass's stage buffers fit in shared memory and the forward input is at
-// most half the padded length (ny <= py/2, the zero padding the first pass relies on).
+// Used when the buffers fit in shared memory and the forward input is at most half the padded
+// length (ny <= py/2, the zero padding the first pass relies on).
 template <typename T, int N>
 mm_status fs_setup_y_tma(ConvPlan *p)
 {
 	using C = cplx<T>;
-	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
-	using GF = YTmaGeom<N, TB, false, C>;
-	using GI = YTmaGeom<N, TB, true, C>;
+	using GF = YTmaGeom<N, false, C>;
+	using GI = YTmaGeom<N, true, C>;
 	p->tma_y = false;
-	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || TB * sizeof(C) < 16) return MM_OK;
+	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || GF::TB * sizeof(C) < 16 || GF::TB * GF::E > 256) return MM_OK;
 	constexpr int E = GF::E;
 	const uint64_t d0 = (uint64_t)p->lx * E, rowb = (uint64_t)p->lx * sizeof(C), planeb = rowb * p->py;
-	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, TB * E, GF::BR, 1));
-	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, TB * E, GI::BR, 1));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, false>, GF::SMEM));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, true>, GI::SMEM));
+	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, GF::TB * E, GF::BR, 1));
+	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, GI::TB * E, GI::BR, 1));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, false>, GF::SMEM));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, true>, GI::SMEM));
 	int bf = 0, bi = 0;
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, TB, false>, THREADS, GF::SMEM));
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, TB, true>, THREADS, GI::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, false>, GF::THREADS, GF::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, true>, GI::THREADS, GI::SMEM));
 	if (bf < 1 || bi < 1) return MM_OK;
 	p->grid_yf = bf * num_sms();
 	p->grid_yi = bi * num_sms();
@@ -780,13 +784,12 @@ template <typename T, int N, bool INV>
 void fs_y_tma(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
-	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
-	using G = YTmaGeom<N, TB, INV, C>;
-	const int tiles_x = (p->hx + TB - 1) / TB, ntiles = tiles_x * 3 * p->nz;
+	using G = YTmaGeom<N, INV, C>;
+	const int tiles_x = (p->hx + G::TB - 1) / G::TB, ntiles = tiles_x * 3 * p->nz;
 	const int grid = std::min(ntiles, INV ? p->grid_yi : p->grid_yf);
-	k_y_tma<T, N, TB, INV><<<grid, THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
-	                                                       INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
-	                                                       (const C *)p->tw_y, p->err);
+	k_y_tma<T, N, INV><<<grid, G::THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
+	                                                      INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
+	                                                      (const C *)p->tw_y, p->err);
 }
 
 template <typename T, int N>

@@ -638,49 +638,42 @@ void fs_z_reg(ConvPlan *p, cudaStream_t st)
 }
 
 // ---- y pass through TMA-staged tiles -------------------------------------------------------------
-// Persistent CTAs walk tiles (TB columns of one (component, z) plane).  A tile's input rows (the
-// ny <= N/2 data rows, padded to N/2 by the TMA unit's zero fill, going forward; all N rows going
-// back) arrive by cp.async.bulk.tensor in one of two buffers while the CTA transforms the previous
-// tile in the other.  The transform runs in place: pass 0 reads the row-major TMA layout and,
-// after a barrier, writes the skewed column layout that the later passes use; the last pass stores
-// straight to HBM, and the buffer is handed back to the TMA unit for the tile after next.  TB
-// columns make 32-byte rows (at least 256 threads for short transforms), so that three CTAs of
-// 256 threads share an SM.  Thread 0 issues the loads; a bounded wait that runs out sets *err and
-// ends the kernel instead of hanging.
-template <int N, bool INV, class C>
+// Persistent CTAs walk tiles (TB columns of one (component, z) plane).  Each tile's input rows
+// (the ny < N/2 data rows padded to N/2 by the TMA unit's zero fill going forward, all N rows
+// going back) arrive by cp.async.bulk.tensor in one of two stage buffers while the previous tile is
+// transformed; pass 0 reads the stage buffer, the later passes work in a skewed shared-memory
+// buffer, and the last pass stores straight to HBM.  Thread 0 issues the loads; a bounded wait that
+// runs out sets *err and ends the kernel instead of hanging.
+template <int N, int TB, bool INV, class C>
 struct YTmaGeom {
-	static constexpr int R = ct_radix(N);
-	static constexpr int TB0 = 32 / (int)sizeof(C), TBT = 256 / (N / R > 0 ? N / R : 1);
-	static constexpr int TB = TB0 > TBT ? TB0 : TBT;
-	static constexpr int THREADS = TB * (N / R);
 	static constexpr int ROWS = INV ? N : N / 2;
 	static constexpr int BR = ROWS < 256 ? ROWS : 256;
 	static constexpr int NBOX = ROWS / BR;
 	static constexpr int E = (int)(sizeof(C) / 8);
 	static constexpr uint32_t TILE_BYTES = (uint32_t)(TB * ROWS * sizeof(C));
-	static constexpr size_t BUF = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 127) / 128 * 128;
-	static constexpr size_t SMEM = 2 * BUF + 16;
-	static constexpr int MINB = (3 * SMEM <= 227 * 1024 && THREADS <= 256) ? 3 : (2 * SMEM <= 227 * 1024 ? 2 : 1);
+	static constexpr size_t WORK = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 15) / 16 * 16;
+	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
 };
 
-template <typename T, int N, bool INV>
-__global__ void __launch_bounds__(YTmaGeom<N, INV, cplx<T>>::THREADS, YTmaGeom<N, INV, cplx<T>>::MINB)
+template <typename T, int N, int TB, bool INV>
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 1)
     k_y_tma(const __grid_constant__ CUtensorMap tmap, cplx<T> *__restrict__ S, int n_out, int hx, int lx,
             int tiles_x, int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
 	using C = cplx<T>;
-	using G = YTmaGeom<N, INV, C>;
-	constexpr int TB = G::TB;
+	using G = YTmaGeom<N, TB, INV, C>;
+	constexpr int R = ct_radix(N);
 	using SI = SmCols<N, TB>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
-	C *buf0 = reinterpret_cast<C *>(smem_tma);
-	C *buf1 = reinterpret_cast<C *>(smem_tma + G::BUF);
-	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
+	C *stage0 = reinterpret_cast<C *>(smem_tma);
+	C *stage1 = stage0 + TB * G::ROWS;
+	C *work = reinterpret_cast<C *>(smem_tma + 2 * (size_t)G::TILE_BYTES);
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * (size_t)G::TILE_BYTES + G::WORK);
 	const int tid = threadIdx.x;
 	const int line = tid & (TB - 1), j0 = tid / TB;
 	auto issue = [&](int t, int b) {
 		const int tx = t % tiles_x, plane = t / tiles_x;
-		C *dst = b ? buf1 : buf0;
+		C *dst = b ? stage1 : stage0;
 		mbar_expect_tx(&bar[b], G::TILE_BYTES);
 #pragma unroll
 		for (int q = 0; q < G::NBOX; ++q)
@@ -710,14 +703,176 @@ __global__ void __launch_bounds__(YTmaGeom<N, INV, cplx<T>>::THREADS, YTmaGeom<N
 		const int kx = tx * TB + line;
 		const bool ok = kx < hx;
 		C *base = S + (size_t)plane * N * lx + (ok ? kx : 0);
-		C *sb = b ? buf1 : buf0;
+		const C *sb = b ? stage1 : stage0;
 		auto ld = [&](int, int r) -> C { return r < G::ROWS ? sb[r * TB + line] : C{0, 0}; };
 		auto st = [&](int, int r, C v) {
 			if (ok && r < n_out) base[(size_t)r * lx] = v;
 		};
-		cta_fft<T, N, G::R, TB, INV, SI, true>(sb, twN, line, j0, ld, st);
-		// hand the buffer back: every thread's generic accesses to it are ordered before the
-		// asynchronous copy that refills it
+		const int next = t + 2 * (int)gridDim.x;
+		auto release = [&]() {
+			__syncthreads();  // every thread has read stage buffer b
+			if (tid == 0 && next < ntiles) {
+				fence_proxy_async();
+				issue(next, b);
+			}
+		};
+		cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
+	}
+}
+
+// ---- x passes through TMA-staged tiles -----------------------------------------------------------
+// Same pipeline as the y pass: persistent CTAs, two buffers, one tile (LPB complex lines = 2 LPB
+// real rows) loading by cp.async.bulk.tensor while the previous one is transformed in place.  A
+// row arrives as xbox_n boxes of xbox_w 8-byte elements, so the staged rows are dense: real rows
+// of nx values going forward, spectrum rows of lx complex values going back.
+template <int N, class C>
+struct XTmaGeom {
+	static constexpr int R = ct_radix(N);
+	static constexpr int LPB = ct_lpb(N, sizeof(C));
+	static constexpr int THREADS = LPB * (N / R);
+	static constexpr size_t WORK = (size_t)SmRows<N, LPB>::SIZE * sizeof(C);
+	// staged rows (at most 2 LPB spectrum rows of N/2 + 1 + padding complex values) fit in WORK
+	// with room to spare for N >= 64; shorter rows use the non-staged kernels
+	static constexpr size_t BUF = (WORK + 127) / 128 * 128;
+	static constexpr size_t SMEM = 2 * BUF + 16;
+	static constexpr int MINB = (3 * SMEM <= 227 * 1024 && THREADS <= 256) ? 3 : (2 * SMEM <= 227 * 1024 ? 2 : 1);
+};
+
+template <typename T, int N, bool SCALE>
+__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB)
+    k_x_fwd_tma(const __grid_constant__ CUtensorMap tmap, const uint8_t *__restrict__ reg,
+                const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny, int nz, int py, int hx,
+                int lx, int ntiles, const cplx<T> *__restrict__ twN, int *err)
+{
+	using C = cplx<T>;
+	using G = XTmaGeom<N, C>;
+	constexpr int LPB = G::LPB, TPL = N / G::R;
+	using SI = SmRows<N, LPB>;
+	extern __shared__ __align__(128) unsigned char smem_tma[];
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
+	const int tid = threadIdx.x;
+	const int line = tid / TPL, j0 = tid % TPL;
+	const int rows = 3 * ny * nz, nyz = ny * nz;
+	const uint32_t tile_bytes = (uint32_t)(2 * LPB * (size_t)nx * sizeof(T));
+	auto issue = [&](int t, int b) {
+		mbar_expect_tx(&bar[b], tile_bytes);
+		tma_load_3d(smem_tma + b * G::BUF, &tmap, 0, 0, t * 2 * LPB, &bar[b]);
+	};
+	if (tid == 0) {
+		mbar_init(&bar[0], 1);
+		mbar_init(&bar[1], 1);
+		fence_proxy_async();
+	}
+	__syncthreads();
+	if (tid == 0) {
+		if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+		if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
+	}
+	uint32_t parity = 0;
+	int k = 0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+		const int b = k & 1;
+		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+		if (__syncthreads_or(late)) {
+			if (tid == 0) atomicExch(err, 1);
+			return;
+		}
+		parity ^= 1u << b;
+		C *sm = reinterpret_cast<C *>(smem_tma + b * G::BUF);
+		const T *rowa = reinterpret_cast<const T *>(sm) + (size_t)(2 * line) * nx;
+		const T *rowb = rowa + nx;
+		const int ra = 2 * (t * LPB + line), rb = ra + 1;
+		const bool va = ra < rows, vb = rb < rows;
+		const int qa = va ? ra : 0, qb = vb ? rb : 0;
+		const uint8_t *Ra = reg ? reg + (size_t)(qa % nyz) * nx : nullptr;
+		const uint8_t *Rb = reg ? reg + (size_t)(qb % nyz) * nx : nullptr;
+		auto ld = [&](int, int x) -> C {
+			T a = 0, bb = 0;
+			if (x < nx) {
+				if (va) { a = rowa[x]; if (SCALE) a *= ms_tab[Ra ? Ra[x] : 0]; }
+				if (vb) { bb = rowb[x]; if (SCALE) bb *= ms_tab[Rb ? Rb[x] : 0]; }
+			}
+			return C{a, bb};
+		};
+		auto st = [&](int l, int kk, C v) { sm[SI::at(l, kk)] = v; };
+		cta_fft<T, N, G::R, LPB, false, SI, true>(sm, twN, line, j0, ld, st);
+		__syncthreads();
+		C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
+		C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
+		const T h = T(0.5);
+		for (int kk = j0; kk < hx; kk += TPL) {
+			const C zk = sm[SI::at(line, kk)], zn = sm[SI::at(line, (N - kk) & (N - 1))];
+			if (va) Sa[kk] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
+			if (vb) Sb[kk] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
+		}
+		const int next = t + 2 * (int)gridDim.x;
+		fence_proxy_async();
+		__syncthreads();
+		if (tid == 0 && next < ntiles) issue(next, b);
+	}
+}
+
+// x inverse: the 2 LPB spectrum rows of a tile lie in one (component, z) plane (ny a multiple of
+// 2 LPB); the 4-D tensor map addresses them as (box element, box, y, plane).
+template <typename T, int N>
+__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB)
+    k_x_inv_tma(const __grid_constant__ CUtensorMap tmap, T *__restrict__ H, int nx, int ny, int hx, int lx,
+                int ntiles, const cplx<T> *__restrict__ twN, int *err)
+{
+	using C = cplx<T>;
+	using G = XTmaGeom<N, C>;
+	constexpr int LPB = G::LPB, TPL = N / G::R;
+	using SI = SmRows<N, LPB>;
+	extern __shared__ __align__(128) unsigned char smem_tma[];
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
+	const int tid = threadIdx.x;
+	const int line = tid / TPL, j0 = tid % TPL;
+	const uint32_t tile_bytes = (uint32_t)(2 * LPB * (size_t)lx * sizeof(C));
+	auto issue = [&](int t, int b) {
+		const int row0 = t * 2 * LPB;
+		mbar_expect_tx(&bar[b], tile_bytes);
+		tma_load_4d(smem_tma + b * G::BUF, &tmap, 0, 0, row0 % ny, row0 / ny, &bar[b]);
+	};
+	if (tid == 0) {
+		mbar_init(&bar[0], 1);
+		mbar_init(&bar[1], 1);
+		fence_proxy_async();
+	}
+	__syncthreads();
+	if (tid == 0) {
+		if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
+		if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
+	}
+	uint32_t parity = 0;
+	int k = 0;
+	for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
+		const int b = k & 1;
+		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+		if (__syncthreads_or(late)) {
+			if (tid == 0) atomicExch(err, 1);
+			return;
+		}
+		parity ^= 1u << b;
+		C *sm = reinterpret_cast<C *>(smem_tma + b * G::BUF);
+		const C *Sa = sm + (size_t)(2 * line) * lx;
+		const C *Sb = Sa + lx;
+		const size_t ra = 2 * ((size_t)t * LPB + line);
+		T *Ha = H + ra * nx, *Hb = Ha + nx;
+		auto ld = [&](int, int f) -> C {
+			const bool mirror = f >= hx;
+			const int ff = mirror ? N - f : f;
+			C A = Sa[ff], B = Sb[ff];
+			if (ff == 0 || 2 * ff == N) { A.y = 0; B.y = 0; }
+			if (mirror) { A.y = -A.y; B.y = -B.y; }
+			return C{A.x - B.y, A.y + B.x};
+		};
+		auto st = [&](int, int x, C v) {
+			if (x < nx) {
+				Ha[x] = v.x;
+				Hb[x] = v.y;
+			}
+		};
+		cta_fft<T, N, G::R, LPB, true, SI, true>(sm, twN, line, j0, ld, st);
 		const int next = t + 2 * (int)gridDim.x;
 		fence_proxy_async();
 		__syncthreads();
@@ -750,25 +905,26 @@ mm_status fs_setup_len()
 }
 
 // TMA-staged y passes: tensor maps over the spectrum, shared-memory size, persistent grid size.
-// Used when the buffers fit in shared memory and the forward input is at most half the padded
-// length (ny <= py/2, the zero padding the first pass relies on).
+// Used when the inverse pass's stage buffers fit in shared memory and the forward input is at
+// most half the padded length (ny <= py/2, the zero padding the first pass relies on).
 template <typename T, int N>
 mm_status fs_setup_y_tma(ConvPlan *p)
 {
 	using C = cplx<T>;
-	using GF = YTmaGeom<N, false, C>;
-	using GI = YTmaGeom<N, true, C>;
+	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	using GF = YTmaGeom<N, TB, false, C>;
+	using GI = YTmaGeom<N, TB, true, C>;
 	p->tma_y = false;
-	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || GF::TB * sizeof(C) < 16 || GF::TB * GF::E > 256) return MM_OK;
+	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || TB * sizeof(C) < 16) return MM_OK;
 	constexpr int E = GF::E;
 	const uint64_t d0 = (uint64_t)p->lx * E, rowb = (uint64_t)p->lx * sizeof(C), planeb = rowb * p->py;
-	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, GF::TB * E, GF::BR, 1));
-	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, GI::TB * E, GI::BR, 1));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, false>, GF::SMEM));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, true>, GI::SMEM));
+	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, TB * E, GF::BR, 1));
+	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, TB * E, GI::BR, 1));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, false>, GF::SMEM));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, true>, GI::SMEM));
 	int bf = 0, bi = 0;
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, false>, GF::THREADS, GF::SMEM));
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, true>, GI::THREADS, GI::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, TB, false>, THREADS, GF::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, TB, true>, THREADS, GI::SMEM));
 	if (bf < 1 || bi < 1) return MM_OK;
 	p->grid_yf = bf * num_sms();
 	p->grid_yi = bi * num_sms();
@@ -784,12 +940,113 @@ template <typename T, int N, bool INV>
 void fs_y_tma(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
-	using G = YTmaGeom<N, INV, C>;
-	const int tiles_x = (p->hx + G::TB - 1) / G::TB, ntiles = tiles_x * 3 * p->nz;
+	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	using G = YTmaGeom<N, TB, INV, C>;
+	const int tiles_x = (p->hx + TB - 1) / TB, ntiles = tiles_x * 3 * p->nz;
 	const int grid = std::min(ntiles, INV ? p->grid_yi : p->grid_yf);
-	k_y_tma<T, N, INV><<<grid, G::THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
-	                                                      INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
-	                                                      (const C *)p->tw_y, p->err);
+	k_y_tma<T, N, TB, INV><<<grid, THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
+	                                                       INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
+	                                                       (const C *)p->tw_y, p->err);
+}
+
+// TMA-staged x passes.  The inverse pass's tensor map (over the spectrum) is fixed; the forward
+// pass reads the state the caller passes, so its map is encoded per input pointer (a small cache
+// keeps the solver's few state buffers).
+template <typename T, int N>
+mm_status fs_setup_x_tma(ConvPlan *p)
+{
+	using C = cplx<T>;
+	using G = XTmaGeom<N, C>;
+	constexpr int LPB = G::LPB;
+	p->tma_xf = p->tma_xi = false;
+	if (G::SMEM > 227 * 1024 || N < 64) return MM_OK;
+	int occ = 0;
+	// forward: dense real rows split into boxes of even width
+	const size_t wf = (size_t)p->nx * sizeof(T) / 8;
+	const size_t nbf = (wf + 255) / 256;
+	if ((p->nx * sizeof(T)) % 16 == 0 && wf % (2 * nbf) == 0 && 2 * LPB * p->nx * sizeof(T) <= G::BUF) {
+		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, false>, G::SMEM));
+		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, true>, G::SMEM));
+		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_fwd_tma<T, N, true>, G::THREADS, G::SMEM));
+		if (occ >= 1) {
+			p->grid_xf = occ * num_sms();
+			p->xf_box_n = (int)nbf;
+			p->xf_box_w = (int)(wf / nbf);
+			p->tma_xf = true;
+		}
+	}
+	// inverse: spectrum rows of a tile within one plane
+	if (p->ny % (2 * LPB) == 0 && (size_t)2 * LPB * p->lx * sizeof(C) <= G::BUF) {
+		const uint64_t rowb = (uint64_t)p->lx * sizeof(C);
+		const uint64_t dims[4] = {(uint64_t)p->xbox_w, (uint64_t)p->xbox_n, (uint64_t)p->ny, 3ull * p->nz};
+		const uint64_t strides[3] = {(uint64_t)p->xbox_w * 8, rowb, rowb * p->py};
+		const uint32_t box[4] = {(uint32_t)p->xbox_w, (uint32_t)p->xbox_n, (uint32_t)(2 * LPB), 1};
+		MM_TRY(tma_encode(&p->tm_xi, p->spec, 4, dims, strides, box));
+		MM_TRY(set_smem<T>((const void *)k_x_inv_tma<T, N>, G::SMEM));
+		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_inv_tma<T, N>, G::THREADS, G::SMEM));
+		if (occ >= 1) {
+			p->grid_xi = occ * num_sms();
+			p->tma_xi = true;
+		}
+	}
+	if ((p->tma_xf || p->tma_xi) && !p->err) {
+		MM_CUDA(cudaMalloc(&p->err, sizeof(int)));
+		MM_CUDA(cudaMemset(p->err, 0, sizeof(int)));
+	}
+	return MM_OK;
+}
+
+// Tensor map of the forward x pass over the real rows at M (NULL when M is not 16-byte aligned).
+template <typename T>
+const CUtensorMap *x_fwd_map(ConvPlan *p, const T *M, int lpb)
+{
+	if (reinterpret_cast<uintptr_t>(M) & 15) return nullptr;
+	for (int i = 0; i < ConvPlan::XF_CACHE; ++i)
+		if (p->xf_ptr[i] == M) return &p->xf_map[i];
+	const int slot = p->xf_next;
+	const uint64_t rows = 3ull * p->ny * p->nz;
+	const uint64_t dims[3] = {(uint64_t)p->xf_box_w, (uint64_t)p->xf_box_n, rows};
+	const uint64_t strides[2] = {(uint64_t)p->xf_box_w * 8, (uint64_t)p->nx * sizeof(T)};
+	const uint32_t box[3] = {(uint32_t)p->xf_box_w, (uint32_t)p->xf_box_n, (uint32_t)(2 * lpb)};
+	if (tma_encode(&p->xf_map[slot], M, 3, dims, strides, box) != MM_OK) {
+		clear_error();
+		return nullptr;
+	}
+	p->xf_ptr[slot] = M;
+	p->xf_next = (slot + 1) % ConvPlan::XF_CACHE;
+	return &p->xf_map[slot];
+}
+
+template <typename T, int N>
+bool fs_x_fwd_tma(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, cudaStream_t st)
+{
+	using C = cplx<T>;
+	using G = XTmaGeom<N, C>;
+	const CUtensorMap *map = x_fwd_map<T>(p, M, G::LPB);
+	if (!map) return false;
+	const int lines = (3 * p->ny * p->nz + 1) / 2;
+	const int ntiles = (lines + G::LPB - 1) / G::LPB;
+	const int grid = std::min(ntiles, p->grid_xf);
+	if (ms_tab)
+		k_x_fwd_tma<T, N, true><<<grid, G::THREADS, G::SMEM, st>>>(*map, reg, ms_tab, (C *)p->spec, p->nx, p->ny,
+		                                                            p->nz, p->py, p->hx, p->lx, ntiles,
+		                                                            (const C *)p->tw_x, p->err);
+	else
+		k_x_fwd_tma<T, N, false><<<grid, G::THREADS, G::SMEM, st>>>(*map, reg, ms_tab, (C *)p->spec, p->nx, p->ny,
+		                                                             p->nz, p->py, p->hx, p->lx, ntiles,
+		                                                             (const C *)p->tw_x, p->err);
+	return true;
+}
+
+template <typename T, int N>
+void fs_x_inv_tma(ConvPlan *p, T *H, cudaStream_t st)
+{
+	using C = cplx<T>;
+	using G = XTmaGeom<N, C>;
+	const int ntiles = 3 * p->ny * p->nz / (2 * G::LPB);
+	const int grid = std::min(ntiles, p->grid_xi);
+	k_x_inv_tma<T, N><<<grid, G::THREADS, G::SMEM, st>>>(p->tm_xi, H, p->nx, p->ny, p->hx, p->lx, ntiles,
+	                                                     (const C *)p->tw_x, p->err);
 }
 
 template <typename T, int N>
@@ -867,6 +1124,9 @@ mm_status fs_setup(ConvPlan *p)
 	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_SETUP); MM_TRY(r); }
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_SETUP); MM_TRY(r); }
 #undef MM_SETUP
+#define MM_XTSETUP(N) r = fs_setup_x_tma<T, N>(p)
+	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_XTSETUP); MM_TRY(r); }
+#undef MM_XTSETUP
 #define MM_YTSETUP(N) r = fs_setup_y_tma<T, N>(p)
 	if (p->fast_y) { MM_FS_SWITCH(p->py, MM_YTSETUP); MM_TRY(r); }
 #undef MM_YTSETUP
@@ -1008,7 +1268,14 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	const double ypad = 3.0 * p->hx * p->py * p->nz * c;      // y-transformed, z < nz
 	const double tens = 6.0 * p->hx * p->qy * p->qz * s;
 	ProfToken tk = prof_begin(st);
-	if (p->fast_x) {
+	bool staged = false;
+	if (p->tma_xf) {
+#define MM_XTF(N) staged = fs_x_fwd_tma<T, N>(p, M, reg, ms_tab, st)
+		MM_FS_SWITCH(p->px, MM_XTF);
+#undef MM_XTF
+	}
+	if (staged) {
+	} else if (p->fast_x) {
 #define MM_XF(N) fs_x_fwd<T, N>(p, M, reg, ms_tab, st)
 		MM_FS_SWITCH(p->px, MM_XF);
 #undef MM_XF
@@ -1083,7 +1350,11 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		prof_end(tk, "k_y_inv", half + ypad, st);
 	}
 	tk = prof_begin(st);
-	if (p->fast_x) {
+	if (p->tma_xi) {
+#define MM_XTI(N) fs_x_inv_tma<T, N>(p, H, st)
+		MM_FS_SWITCH(p->px, MM_XTI);
+#undef MM_XTI
+	} else if (p->fast_x) {
 #define MM_XI(N) fs_x_inv<T, N>(p, H, st)
 		MM_FS_SWITCH(p->px, MM_XI);
 #undef MM_XI
@@ -1117,8 +1388,8 @@ size_t ConvPlan::spec_bytes() const
 	return c * 3 * (size_t)nz * py * lx;
 }
 
-mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
-                        uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2)
+mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
+                     const uint32_t *box)
 {
 	using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
 	                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -1134,18 +1405,34 @@ mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_
 		}
 		encode = reinterpret_cast<Encode>(fn);
 	}
-	if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride1 & 15) || (stride2 & 15) || ((b0 * 8) & 15))
+	if (rank < 1 || rank > 5 || (reinterpret_cast<uintptr_t>(base) & 15) || ((box[0] * 8) & 15))
 		return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map not 16-byte aligned");
-	const cuuint64_t dims[3] = {d0, d1, d2};
-	const cuuint64_t strides[2] = {stride1, stride2};
-	const cuuint32_t box[3] = {b0, b1, b2};
-	const cuuint32_t estr[3] = {1, 1, 1};
-	const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, const_cast<void *>(base), dims, strides, box,
-	                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+	cuuint64_t d[5], sb[4];
+	cuuint32_t bx[5], estr[5];
+	for (int i = 0; i < rank; ++i) {
+		d[i] = dims[i];
+		bx[i] = box[i];
+		estr[i] = 1;
+		if (box[i] < 1 || box[i] > 256) return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map box beyond 256");
+	}
+	for (int i = 0; i + 1 < rank; ++i) {
+		sb[i] = strides[i];
+		if (strides[i] & 15) return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map stride not 16-byte aligned");
+	}
+	const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, const_cast<void *>(base), d, sb,
+	                          bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
 	                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 	if (r != CUDA_SUCCESS)
 		return fail(MM_ERR_CUDA, "conv: cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
 	return MM_OK;
+}
+
+mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
+                        uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2)
+{
+	const uint64_t dims[3] = {d0, d1, d2}, strides[2] = {stride1, stride2};
+	const uint32_t box[3] = {b0, b1, b2};
+	return tma_encode(map, base, 3, dims, strides, box);
 }
 
 ConvPlan::~ConvPlan()
@@ -1171,7 +1458,17 @@ mm_status conv_plan_create(ConvPlan **out, int prec, int nx, int ny, int nz, int
 	p->nx = nx; p->ny = ny; p->nz = nz;
 	p->px = px; p->py = py; p->pz = pz;
 	p->hx = px / 2 + 1;
-	p->lx = (prec == MM_F32) ? (p->hx + 1) & ~1 : p->hx;
+	{
+		// row stride: 8-byte elements per row a multiple of 2 * xbox_n, so that a row splits into
+		// xbox_n TMA boxes of xbox_w (even, <= 256) elements with 16-byte aligned rows
+		const int E = prec == MM_F32 ? 1 : 2;
+		int w = p->hx * E;
+		const int nb = (w + 255) / 256;
+		w = (w + 2 * nb - 1) / (2 * nb) * (2 * nb);
+		p->lx = w / E;
+		p->xbox_n = nb;
+		p->xbox_w = w / nb;
+	}
 	p->qy = py / 2 + 1;
 	p->qz = pz / 2 + 1;
 	p->is2d = (nz == 1 && pz == 1);

@@ -13,7 +13,8 @@ struct ConvPlan {
 	int nx = 0, ny = 0, nz = 0;     // grid
 	int px = 0, py = 0, pz = 0;     // padded (FFT) lengths
 	int hx = 0;                     // px/2 + 1 stored x frequencies
-	int lx = 0;                     // spectrum row stride (hx, rounded up to even in FP32: 16-byte rows)
+	int lx = 0;                     // spectrum row stride (>= hx complex, rows 16-byte aligned)
+	int xbox_n = 1, xbox_w = 0;     // a spectrum row as xbox_n TMA boxes of xbox_w 8-byte elements
 	int qy = 0, qz = 0;             // py/2 + 1, pz/2 + 1 stored tensor frequencies
 	bool is2d = false;              // nz == 1 && pz == 1
 	bool fast_x = false, fast_y = false, fast_z = false;  // power-of-two register-FFT passes
@@ -22,6 +23,14 @@ struct ConvPlan {
 	CUtensorMap tm_yf{}, tm_yi{};   // spectrum views of the forward (ny rows) and inverse (py rows) y pass
 	int grid_yf = 0, grid_yi = 0;   // persistent grid sizes of those passes
 	int *err = nullptr;             // device word set when a bounded wait of a staged pass gave up
+	bool tma_xf = false, tma_xi = false;  // x passes fed by TMA-staged tiles
+	int grid_xf = 0, grid_xi = 0;
+	int xf_box_n = 1, xf_box_w = 0;       // a real input row as boxes of 8-byte elements
+	CUtensorMap tm_xi{};                  // spectrum rows y < ny of each plane, for the inverse x pass
+	static constexpr int XF_CACHE = 4;    // forward-pass maps, one per input buffer seen
+	const void *xf_ptr[XF_CACHE] = {};
+	CUtensorMap xf_map[XF_CACHE] = {};
+	int xf_next = 0;
 	FftRadices rx{}, ry{}, rz{};
 	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
 	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]

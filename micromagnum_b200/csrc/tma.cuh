@@ -17,6 +17,9 @@ namespace mm {
 // Out-of-range elements of a box read as zero.
 mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_t d1, uint64_t d2,
                         uint64_t stride1, uint64_t stride2, uint32_t b0, uint32_t b1, uint32_t b2);
+// Same for rank 1..5: dims[0] fastest, strides[] in bytes of dims 1..rank-1.
+mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
+                     const uint32_t *box);
 
 // Spin limit of a bounded mbarrier wait (each try_wait already blocks for a while in hardware);
 // a wait that exceeds it reports a timeout instead of hanging the GPU.
@@ -61,6 +64,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 		if (done) return true;
 	}
 	return false;
+}
+
+// 2-D, 3-D and 4-D tiled loads of one box into shared memory, completing on `bar` (transaction
+// bytes).
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar)
+{
+	asm volatile(
+	    "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+	    "[%4];" ::"r"(smem_u32(dst)),
+	    "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+	    : "memory");
+}
+
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, int c0, int c1, int c2, int c3,
+                                            uint64_t *bar)
+{
+	asm volatile(
+	    "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+	    "%5}], [%6];" ::"r"(smem_u32(dst)),
+	    "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
+	    : "memory");
 }
 
 // 3-D tiled load of one box into shared memory, completing on `bar` (transaction bytes).

@@ -734,13 +734,16 @@ struct XTmaGeom {
 	// staged rows (at most 2 LPB spectrum rows of N/2 + 1 + padding complex values) fit in WORK
 	// with room to spare for N >= 64; shorter rows use the non-staged kernels
 	static constexpr size_t BUF = (WORK + 127) / 128 * 128;
-	static constexpr size_t SMEM = 2 * BUF + 16;
+	static constexpr size_t SMEM = 2 * BUF + 16 + 256 * (sizeof(C) / 2);  // + the forward pass's Ms table
 	static constexpr int MINB = (3 * SMEM <= 227 * 1024 && THREADS <= 256) ? 3 : (2 * SMEM <= 227 * 1024 ? 2 : 1);
 };
 
+// Forward: with SCALE the tile's region bytes (rows r % (ny nz), contiguous within a tile) ride
+// along in the same buffer behind the real rows, and the 256-entry Ms table sits in shared memory,
+// so that pass 0 reads nothing but shared memory.
 template <typename T, int N, bool SCALE>
 __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB)
-    k_x_fwd_tma(const __grid_constant__ CUtensorMap tmap, const uint8_t *__restrict__ reg,
+    k_x_fwd_tma(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap rmap,
                 const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny, int nz, int py, int hx,
                 int lx, int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
@@ -750,14 +753,19 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 	using SI = SmRows<N, LPB>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
 	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
+	T *msr = reinterpret_cast<T *>(smem_tma + 2 * G::BUF + 16);
 	const int tid = threadIdx.x;
 	const int line = tid / TPL, j0 = tid % TPL;
 	const int rows = 3 * ny * nz, nyz = ny * nz;
-	const uint32_t tile_bytes = (uint32_t)(2 * LPB * (size_t)nx * sizeof(T));
+	const uint32_t row_bytes = (uint32_t)(2 * LPB * (size_t)nx * sizeof(T));
+	const uint32_t tile_bytes = row_bytes + (SCALE ? (uint32_t)(2 * LPB * nx) : 0u);
 	auto issue = [&](int t, int b) {
 		mbar_expect_tx(&bar[b], tile_bytes);
 		tma_load_3d(smem_tma + b * G::BUF, &tmap, 0, 0, t * 2 * LPB, &bar[b]);
+		if (SCALE) tma_load_2d(smem_tma + b * G::BUF + row_bytes, &rmap, 0, (t * 2 * LPB) % nyz, &bar[b]);
 	};
+	if (SCALE)
+		for (int r = tid; r < 256; r += blockDim.x) msr[r] = ms_tab[r];
 	if (tid == 0) {
 		mbar_init(&bar[0], 1);
 		mbar_init(&bar[1], 1);
@@ -781,16 +789,16 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 		C *sm = reinterpret_cast<C *>(smem_tma + b * G::BUF);
 		const T *rowa = reinterpret_cast<const T *>(sm) + (size_t)(2 * line) * nx;
 		const T *rowb = rowa + nx;
+		const uint8_t *rga = smem_tma + b * G::BUF + row_bytes + (size_t)(2 * line) * nx;
+		const uint8_t *rgb = rga + nx;
 		const int ra = 2 * (t * LPB + line), rb = ra + 1;
 		const bool va = ra < rows, vb = rb < rows;
 		const int qa = va ? ra : 0, qb = vb ? rb : 0;
-		const uint8_t *Ra = reg ? reg + (size_t)(qa % nyz) * nx : nullptr;
-		const uint8_t *Rb = reg ? reg + (size_t)(qb % nyz) * nx : nullptr;
 		auto ld = [&](int, int x) -> C {
 			T a = 0, bb = 0;
 			if (x < nx) {
-				if (va) { a = rowa[x]; if (SCALE) a *= ms_tab[Ra ? Ra[x] : 0]; }
-				if (vb) { bb = rowb[x]; if (SCALE) bb *= ms_tab[Rb ? Rb[x] : 0]; }
+				if (va) { a = rowa[x]; if (SCALE) a *= msr[rga[x]]; }
+				if (vb) { bb = rowb[x]; if (SCALE) bb *= msr[rgb[x]]; }
 			}
 			return C{a, bb};
 		};
@@ -965,6 +973,9 @@ mm_status fs_setup_x_tma(ConvPlan *p)
 	const size_t wf = (size_t)p->nx * sizeof(T) / 8;
 	const size_t nbf = (wf + 255) / 256;
 	if ((p->nx * sizeof(T)) % 16 == 0 && wf % (2 * nbf) == 0 && 2 * LPB * p->nx * sizeof(T) <= G::BUF) {
+		// region bytes ride behind the rows when a tile's rows are contiguous in the region map
+		p->tma_xf_scale = p->nx % 16 == 0 && (p->ny * p->nz) % (2 * LPB) == 0 && p->nx / 8 <= 256 &&
+		                  2 * LPB * p->nx * (sizeof(T) + 1) <= G::BUF;
 		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, false>, G::SMEM));
 		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, true>, G::SMEM));
 		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_fwd_tma<T, N, true>, G::THREADS, G::SMEM));
@@ -997,6 +1008,22 @@ mm_status fs_setup_x_tma(ConvPlan *p)
 }
 
 // Tensor map of the forward x pass over the real rows at M (NULL when M is not 16-byte aligned).
+// Tensor map of the region bytes of the forward x pass (NULL when not usable for `reg`).
+const CUtensorMap *x_reg_map(ConvPlan *p, const uint8_t *reg, int lpb)
+{
+	if (!p->tma_xf_scale || !reg || (reinterpret_cast<uintptr_t>(reg) & 15)) return nullptr;
+	if (p->xr_ptr == reg) return &p->xr_map;
+	const uint64_t dims[2] = {(uint64_t)p->nx / 8, (uint64_t)p->ny * p->nz};
+	const uint64_t strides[1] = {(uint64_t)p->nx};
+	const uint32_t box[2] = {(uint32_t)(p->nx / 8), (uint32_t)(2 * lpb)};
+	if (tma_encode(&p->xr_map, reg, 2, dims, strides, box) != MM_OK) {
+		clear_error();
+		return nullptr;
+	}
+	p->xr_ptr = reg;
+	return &p->xr_map;
+}
+
 template <typename T>
 const CUtensorMap *x_fwd_map(ConvPlan *p, const T *M, int lpb)
 {
@@ -1024,15 +1051,21 @@ bool fs_x_fwd_tma(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	using G = XTmaGeom<N, C>;
 	const CUtensorMap *map = x_fwd_map<T>(p, M, G::LPB);
 	if (!map) return false;
+	const CUtensorMap *rmap = map;
+	if (ms_tab) {
+		// a missing region map means region 0 everywhere: the staged kernel needs real bytes
+		rmap = reg ? x_reg_map(p, reg, G::LPB) : nullptr;
+		if (!rmap) return false;
+	}
 	const int lines = (3 * p->ny * p->nz + 1) / 2;
 	const int ntiles = (lines + G::LPB - 1) / G::LPB;
 	const int grid = std::min(ntiles, p->grid_xf);
 	if (ms_tab)
-		k_x_fwd_tma<T, N, true><<<grid, G::THREADS, G::SMEM, st>>>(*map, reg, ms_tab, (C *)p->spec, p->nx, p->ny,
+		k_x_fwd_tma<T, N, true><<<grid, G::THREADS, G::SMEM, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
 		                                                            p->nz, p->py, p->hx, p->lx, ntiles,
 		                                                            (const C *)p->tw_x, p->err);
 	else
-		k_x_fwd_tma<T, N, false><<<grid, G::THREADS, G::SMEM, st>>>(*map, reg, ms_tab, (C *)p->spec, p->nx, p->ny,
+		k_x_fwd_tma<T, N, false><<<grid, G::THREADS, G::SMEM, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
 		                                                             p->nz, p->py, p->hx, p->lx, ntiles,
 		                                                             (const C *)p->tw_x, p->err);
 	return true;

@@ -24,6 +24,7 @@ struct ConvPlan {
 	int grid_yf = 0, grid_yi = 0;   // persistent grid sizes of those passes
 	int *err = nullptr;             // device word set when a bounded wait of a staged pass gave up
 	bool tma_xf = false, tma_xi = false;  // x passes fed by TMA-staged tiles
+	bool tma_xf_scale = false;            // ... also with the Ms[region] input scale
 	int grid_xf = 0, grid_xi = 0;
 	int xf_box_n = 1, xf_box_w = 0;       // a real input row as boxes of 8-byte elements
 	CUtensorMap tm_xi{};                  // spectrum rows y < ny of each plane, for the inverse x pass
@@ -31,6 +32,8 @@ struct ConvPlan {
 	const void *xf_ptr[XF_CACHE] = {};
 	CUtensorMap xf_map[XF_CACHE] = {};
 	int xf_next = 0;
+	const void *xr_ptr = nullptr;         // region map the region tensor map was encoded for
+	CUtensorMap xr_map{};                 // region bytes of the forward pass's rows
 	FftRadices rx{}, ry{}, rz{};
 	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
 	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]
@@ -50,7 +53,7 @@ struct ConvPlan {
 mm_status conv_plan_create(ConvPlan **out, int prec, int nx, int ny, int nz, int px, int py,
                            int pz, const double *N_device, cudaStream_t st);
 
-// H = N * (Ms[region] * M) when regions/ms_table are given, else H = N * M.
+// H = N * (Ms[region] * M) when regions/ms_table are given (ms_table: 256 entries), else H = N * M.
 // M and H are SoA arrays of T (T = double for MM_F64, float for MM_F32).
 mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const void *ms_table,
                        void *H, cudaStream_t st);

@@ -560,7 +560,7 @@ struct mm_solver {
 	Tableau tab{};
 	ConvPlan *conv = nullptr;
 	void *mat = nullptr;           // DevMat<T>[nmat]
-	void *ms_tab = nullptr;        // T[nmat] (Ms per region, for the demag input)
+	void *ms_tab = nullptr;        // T[256] (Ms per region, zero past nmat; the demag input scale)
 	uint8_t *reg = nullptr;
 	void *m = nullptr, *m_lo = nullptr;        // state (unit), low part (F32)
 	void *ys[2] = {nullptr, nullptr};          // stage state ping-pong
@@ -661,7 +661,8 @@ mm_status build_materials(mm_solver *s, int nmat, const mm_material *mats)
 	}
 	MM_CUDA(cudaMalloc(&s->mat, sizeof(DevMat<T>) * nmat));
 	MM_CUDA(cudaMemcpy(s->mat, h.data(), sizeof(DevMat<T>) * nmat, cudaMemcpyHostToDevice));
-	MM_CUDA(cudaMalloc(&s->ms_tab, sizeof(T) * nmat));
+	MM_CUDA(cudaMalloc(&s->ms_tab, sizeof(T) * 256));  // full 8-bit region range, zero past nmat
+	MM_CUDA(cudaMemset(s->ms_tab, 0, sizeof(T) * 256));
 	MM_CUDA(cudaMemcpy(s->ms_tab, ms.data(), sizeof(T) * nmat, cudaMemcpyHostToDevice));
 	return MM_OK;
 }

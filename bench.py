@@ -203,7 +203,7 @@ def run_ours(args, rank, world, local_rank):
     reg, axes = grains(DIMS, NGRAINS, SEED)
     M0 = initial_M(n, SEED + rank)
     s = Solver(RectangularMesh(DIMS, DELTA), materials(axes), regions=reg,
-               terms=("demag", "exchange", "uniaxial", "zhangli"), precision="f32", evolver="dp54",
+               terms=("demag", "exchange", "uniaxial", "zhangli"), precision=args.precision, evolver="dp54",
                eps_abs=1e-3, eps_rel=1e-4)
     s.M = M0
     for _ in range(args.warmup):
@@ -293,7 +293,8 @@ def run_ours(args, rank, world, local_rank):
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (compensated state; f64 tensor set-up and step control)",
+            "scaling": "weak", "vs_baseline": None, "dtype": ("f32 (compensated state; f64 tensor set-up and step control)" if args.precision == "f32"
+                      else "f64 (plain mode)"),
             "data": "synthetic (seeded grains, axes, initial m)",
             "config": {"workload": WORKLOAD, "cells": n, "rhs_evals": evals, "accepted_steps": steps,
                        "attempts": attempts, "parallelism": f"{world} independent replicas (one slab per GPU)",
@@ -364,6 +365,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", choices=["f32", "f64"], default="f32",
+                    help="f32: the compensated single-precision form (default); f64: the plain mode")
     ap.add_argument("--dims", default=None, help="override the grid, e.g. 512,512,8 (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:

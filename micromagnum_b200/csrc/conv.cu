@@ -407,18 +407,19 @@ __host__ __device__ constexpr int ct_lpb(int n, int csize)
 }
 
 // y pass (3-D): TB columns per CTA; forward pads rows n_in -> N, inverse crops N -> n_out.
+// (bx: column tile, plane = c nz + z; shared by the single-grid and the grouped kernels)
 template <typename T, int N, int TB, bool INV>
-__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
-                                                                 int hx, int lx, const cplx<T> *__restrict__ twN)
+__device__ __forceinline__ void y_ct_body(cplx<T> *__restrict__ S, int n_in, int n_out, int hx, int lx,
+                                          const cplx<T> *__restrict__ twN, int bx, int plane)
 {
 	using C = cplx<T>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *sm = reinterpret_cast<C *>(smem_raw);
 	const int tid = threadIdx.x;
 	const int line = tid & (TB - 1), j0 = tid / TB;
-	const int kx = blockIdx.x * TB + line;
+	const int kx = bx * TB + line;
 	const bool ok = kx < hx;
-	C *base = S + (size_t)(blockIdx.z * nz + blockIdx.y) * N * lx + (ok ? kx : 0);
+	C *base = S + (size_t)plane * N * lx + (ok ? kx : 0);
 	auto ld = [&](int, int k) -> C { return (ok && k < n_in) ? base[(size_t)k * lx] : C{0, 0}; };
 	auto st = [&](int, int k, C v) {
 		if (ok && k < n_out) base[(size_t)k * lx] = v;
@@ -426,13 +427,18 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__r
 	cta_fft<T, N, ct_radix(N), TB, INV, SmCols<N, TB>>(sm, twN, line, j0, ld, st);
 }
 
+template <typename T, int N, int TB, bool INV>
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__restrict__ S, int n_in, int n_out, int nz,
+                                                                 int hx, int lx, const cplx<T> *__restrict__ twN)
+{
+	y_ct_body<T, N, TB, INV>(S, n_in, n_out, hx, lx, twN, blockIdx.x, blockIdx.z * nz + blockIdx.y);
+}
+
 // x pass forward: LPB complex lines per CTA (line q packs real rows 2q, 2q+1).
 template <typename T, int N, int LPB, bool SCALE>
-__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *__restrict__ M,
-                                                                     const uint8_t *__restrict__ reg,
-                                                                     const T *__restrict__ ms_tab,
-                                                                     cplx<T> *__restrict__ S, int nx, int ny, int nz,
-                                                                     int py, int hx, int lx, const cplx<T> *__restrict__ twN)
+__device__ __forceinline__ void x_fwd_ct_body(const T *__restrict__ M, const uint8_t *__restrict__ reg,
+                                              const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny,
+                                              int nz, int py, int hx, int lx, const cplx<T> *__restrict__ twN, int blk)
 {
 	using C = cplx<T>;
 	constexpr int TPL = N / ct_radix(N);
@@ -442,7 +448,7 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
 	const int tid = threadIdx.x;
 	const int line = tid / TPL, j0 = tid % TPL;
 	const int rows = 3 * ny * nz, nyz = ny * nz;
-	const int ra = 2 * (blockIdx.x * LPB + line), rb = ra + 1;
+	const int ra = 2 * (blk * LPB + line), rb = ra + 1;
 	const bool va = ra < rows, vb = rb < rows;
 	const int qa = va ? ra : 0, qb = vb ? rb : 0;
 	const T *Ma = M + (size_t)qa * nx, *Mb = M + (size_t)qb * nx;
@@ -469,11 +475,20 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
 	}
 }
 
+template <typename T, int N, int LPB, bool SCALE>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *__restrict__ M,
+                                                                     const uint8_t *__restrict__ reg,
+                                                                     const T *__restrict__ ms_tab,
+                                                                     cplx<T> *__restrict__ S, int nx, int ny, int nz,
+                                                                     int py, int hx, int lx, const cplx<T> *__restrict__ twN)
+{
+	x_fwd_ct_body<T, N, LPB, SCALE>(M, reg, ms_tab, S, nx, ny, nz, py, hx, lx, twN, blockIdx.x);
+}
+
 // x pass inverse: half spectra of rows 2q, 2q+1 -> real rows.
 template <typename T, int N, int LPB>
-__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx<T> *__restrict__ S, T *__restrict__ H,
-                                                                     int nx, int ny, int nz, int py, int hx, int lx,
-                                                                     const cplx<T> *__restrict__ twN)
+__device__ __forceinline__ void x_inv_ct_body(const cplx<T> *__restrict__ S, T *__restrict__ H, int nx, int ny,
+                                              int nz, int py, int hx, int lx, const cplx<T> *__restrict__ twN, int blk)
 {
 	using C = cplx<T>;
 	constexpr int TPL = N / ct_radix(N);
@@ -483,7 +498,7 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx
 	const int tid = threadIdx.x;
 	const int line = tid / TPL, j0 = tid % TPL;
 	const int rows = 3 * ny * nz, nyz = ny * nz;
-	const int ra = 2 * (blockIdx.x * LPB + line), rb = ra + 1;
+	const int ra = 2 * (blk * LPB + line), rb = ra + 1;
 	const bool va = ra < rows, vb = rb < rows;
 	const int qa = va ? ra : 0, qb = vb ? rb : 0;
 	const C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
@@ -505,6 +520,14 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx
 		}
 	};
 	cta_fft<T, N, ct_radix(N), LPB, true, SI>(sm, twN, line, j0, ld, st);
+}
+
+template <typename T, int N, int LPB>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_ct(const cplx<T> *__restrict__ S, T *__restrict__ H,
+                                                                     int nx, int ny, int nz, int py, int hx, int lx,
+                                                                     const cplx<T> *__restrict__ twN)
+{
+	x_inv_ct_body<T, N, LPB>(S, H, nx, ny, nz, py, hx, lx, twN, blockIdx.x);
 }
 
 // z pass with the tensor multiply (CTA-Stockham form): lines (c, b) = c * TB + b hold the z
@@ -574,8 +597,8 @@ __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> 
 constexpr int ZR_THREADS = 192;  // 32 kx x 3 components x 2 rows
 
 template <typename T, int PZ>
-__global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
-                                                        int py, int hx, int lx, int qy, int qz)
+__device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz, int py, int hx,
+                                           int lx, int qy, int qz, int bx, int b)
 {
 	using C = cplx<T>;
 	constexpr int H = PZ / 2;
@@ -583,9 +606,9 @@ __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S
 	C *sm = reinterpret_cast<C *>(smem_raw);  // [row][kz][component][32 kx]
 	const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 	const int c = w % 3, r = w / 3;
-	const int b = blockIdx.y, b1 = py - b;
+	const int b1 = py - b;
 	const bool two = b > 0 && b1 != b;
-	const int kx = blockIdx.x * 32 + lane;
+	const int kx = bx * 32 + lane;
 	const bool ok = (r == 0 || two) && kx < hx;
 	const size_t zstride = (size_t)py * lx;
 	C *col = S + ((size_t)c * nz * py + (size_t)(r == 0 ? b : b1)) * lx + kx;
@@ -627,6 +650,13 @@ __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S
 		for (int z = 0; z < H; ++z)
 			if (z < nz) col[z * zstride] = v[brev<PZ>(z)];
 	}
+}
+
+template <typename T, int PZ>
+__global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
+                                                        int py, int hx, int lx, int qy, int qz)
+{
+	z_reg_body<T, PZ>(S, Nt, nz, py, hx, lx, qy, qz, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, int PZ>
@@ -1528,6 +1558,248 @@ mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const
 		return execute<double>(p, (const double *)M, regions, (const double *)ms_table, (double *)H, st);
 	return execute<float>(p, (const float *)M, regions, (const float *)ms_table, (float *)H, st);
 }
+
+// ---- grouped convolution: many plans, one launch per pass and transform length -------------------
+// Every member plan uses the power-of-two passes (register z pass included).  The members' blocks
+// of one pass and one length form a work list (member, block); a member whose `active` flag is 0
+// skips its blocks, so finished instances drop out without rebuilding the lists.
+namespace {
+
+template <typename T>
+struct GDesc {
+	cplx<T> *spec;
+	const T *tensor;
+	const cplx<T> *tw_x, *tw_y;
+	const T *M[3];
+	T *H;
+	const uint8_t *reg;
+	const T *ms_tab;
+	int nx, ny, nz, py, hx, lx, qy, qz;
+};
+
+template <typename T, int N, int LPB>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_grp(const GDesc<T> *__restrict__ d,
+                                                                      const int2 *__restrict__ items, int input,
+                                                                      const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (active && !active[it.x]) return;
+	const GDesc<T> g = d[it.x];
+	x_fwd_ct_body<T, N, LPB, true>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x,
+	                               it.y);
+}
+
+template <typename T, int N, int LPB>
+__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_grp(const GDesc<T> *__restrict__ d,
+                                                                      const int2 *__restrict__ items,
+                                                                      const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (active && !active[it.x]) return;
+	const GDesc<T> g = d[it.x];
+	x_inv_ct_body<T, N, LPB>(g.spec, g.H, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
+}
+
+template <typename T, int N, int TB, bool INV>
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_grp(const GDesc<T> *__restrict__ d,
+                                                                    const int2 *__restrict__ items,
+                                                                    const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (active && !active[it.x]) return;
+	const GDesc<T> g = d[it.x];
+	const int tiles = (g.hx + TB - 1) / TB;
+	y_ct_body<T, N, TB, INV>(g.spec, INV ? N : g.ny, INV ? g.ny : N, g.hx, g.lx, g.tw_y, it.y % tiles, it.y / tiles);
+}
+
+template <typename T, int PZ>
+__global__ void __launch_bounds__(ZR_THREADS, 3) k_z_grp(const GDesc<T> *__restrict__ d, const int2 *__restrict__ items,
+                                                        const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (active && !active[it.x]) return;
+	const GDesc<T> g = d[it.x];
+	const int tiles = (g.hx + 31) / 32;
+	z_reg_body<T, PZ>(g.spec, g.tensor, g.nz, g.py, g.hx, g.lx, g.qy, g.qz, it.y % tiles, it.y / tiles);
+}
+
+} // namespace
+
+struct ConvGroup {
+	int prec = MM_F32;
+	int count = 0;
+	void *desc = nullptr;  // GDesc<T>[count]
+	struct List {
+		int pass;  // 0 x forward, 1 y forward, 2 z, 3 y inverse, 4 x inverse
+		int len;   // transform length of the pass
+		int2 *items;
+		int n;
+	};
+	std::vector<List> lists;
+	~ConvGroup()
+	{
+		cudaFree(desc);
+		for (auto &l : lists) cudaFree(l.items);
+	}
+};
+
+namespace {
+
+template <typename T>
+mm_status group_smem(int pass, int len)
+{
+	using C = cplx<T>;
+	mm_status r = MM_OK;
+	auto xs = [&](auto nc) {
+		constexpr int N = decltype(nc)::value;
+		constexpr int LPB = ct_lpb(N, sizeof(C)), TB = ct_tb(N, sizeof(C));
+		const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
+		if (pass == 0) r = set_smem<T>((const void *)k_x_fwd_grp<T, N, LPB>, sx);
+		if (pass == 4) r = set_smem<T>((const void *)k_x_inv_grp<T, N, LPB>, sx);
+		if (pass == 1) r = set_smem<T>((const void *)k_y_grp<T, N, TB, false>, sy);
+		if (pass == 3) r = set_smem<T>((const void *)k_y_grp<T, N, TB, true>, sy);
+	};
+	if (pass == 2) {
+		const size_t sz = (size_t)2 * len * 96 * sizeof(C);
+		switch (len) {
+		case 2: r = set_smem<T>((const void *)k_z_grp<T, 2>, sz); break;
+		case 4: r = set_smem<T>((const void *)k_z_grp<T, 4>, sz); break;
+		case 8: r = set_smem<T>((const void *)k_z_grp<T, 8>, sz); break;
+		case 16: r = set_smem<T>((const void *)k_z_grp<T, 16>, sz); break;
+		case 32: if constexpr (sizeof(T) == 4) { r = set_smem<T>((const void *)k_z_grp<T, 32>, sz); } break;
+		}
+		return r;
+	}
+#define MM_GS(N) xs(std::integral_constant<int, N>())
+	MM_FS_SWITCH(len, MM_GS);
+#undef MM_GS
+	return r;
+}
+
+template <typename T>
+void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, const int *active, cudaStream_t st)
+{
+	using C = cplx<T>;
+	const GDesc<T> *d = (const GDesc<T> *)g->desc;
+	auto xs = [&](auto nc) {
+		constexpr int N = decltype(nc)::value;
+		constexpr int LPB = ct_lpb(N, sizeof(C)), TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
+		const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
+		if (l.pass == 0) k_x_fwd_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, input, active);
+		if (l.pass == 4) k_x_inv_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, active);
+		if (l.pass == 1) k_y_grp<T, N, TB, false><<<l.n, TB * TPL, sy, st>>>(d, l.items, active);
+		if (l.pass == 3) k_y_grp<T, N, TB, true><<<l.n, TB * TPL, sy, st>>>(d, l.items, active);
+	};
+	if (l.pass == 2) {
+		const size_t sz = (size_t)2 * l.len * 96 * sizeof(C);
+		switch (l.len) {
+		case 2: k_z_grp<T, 2><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
+		case 4: k_z_grp<T, 4><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
+		case 8: k_z_grp<T, 8><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
+		case 16: k_z_grp<T, 16><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
+		case 32: if constexpr (sizeof(T) == 4) { k_z_grp<T, 32><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); } break;
+		}
+		return;
+	}
+#define MM_GL(N) xs(std::integral_constant<int, N>())
+	MM_FS_SWITCH(l.len, MM_GL);
+#undef MM_GL
+}
+
+template <typename T>
+mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaStream_t st)
+{
+	std::vector<GDesc<T>> h(count);
+	std::vector<std::vector<int2>> items[5];
+	std::vector<int> lens[5];
+	auto add = [&](int pass, int len, int member, int blocks) {
+		size_t k = 0;
+		while (k < lens[pass].size() && lens[pass][k] != len) ++k;
+		if (k == lens[pass].size()) {
+			lens[pass].push_back(len);
+			items[pass].emplace_back();
+		}
+		for (int b = 0; b < blocks; ++b) items[pass][k].push_back(make_int2(member, b));
+	};
+	for (int i = 0; i < count; ++i) {
+		const ConvPlan *p = m[i].plan;
+		if (!p || p->prec != g->prec || p->is2d || !p->fast_x || !p->fast_y || !p->reg_z)
+			return fail(MM_ERR_UNSUPPORTED, "conv group: every member needs power-of-two 3-D padding with a register z pass");
+		GDesc<T> &d = h[i];
+		d.spec = (cplx<T> *)p->spec;
+		d.tensor = (const T *)p->tensor;
+		d.tw_x = (const cplx<T> *)p->tw_x;
+		d.tw_y = (const cplx<T> *)p->tw_y;
+		for (int k = 0; k < 3; ++k) d.M[k] = (const T *)m[i].M[k];
+		d.H = (T *)m[i].H;
+		d.reg = m[i].reg;
+		d.ms_tab = (const T *)m[i].ms_tab;
+		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
+		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
+		using C = cplx<T>;
+		int lpb = 1, tb = 1;
+#define MM_GEO(N) (lpb = ct_lpb(N, sizeof(C)), tb = ct_tb(N, sizeof(C)))
+		MM_FS_SWITCH(p->px, MM_GEO);
+		const int xblocks = ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
+		switch (p->py) {
+		case 4: MM_GEO(4); break; case 8: MM_GEO(8); break; case 16: MM_GEO(16); break; case 32: MM_GEO(32); break;
+		case 64: MM_GEO(64); break; case 128: MM_GEO(128); break; case 256: MM_GEO(256); break;
+		case 512: MM_GEO(512); break; case 1024: MM_GEO(1024); break;
+		case 2048: if constexpr (sizeof(T) == 4) { MM_GEO(2048); } break;
+		}
+#undef MM_GEO
+		add(0, p->px, i, xblocks);
+		add(1, p->py, i, (p->hx + tb - 1) / tb * 3 * p->nz);
+		add(2, p->pz, i, (p->hx + 31) / 32 * p->qy);
+		add(3, p->py, i, (p->hx + tb - 1) / tb * 3 * p->nz);
+		add(4, p->px, i, xblocks);
+	}
+	MM_CUDA(cudaMalloc(&g->desc, sizeof(GDesc<T>) * count));
+	MM_CUDA(cudaMemcpyAsync(g->desc, h.data(), sizeof(GDesc<T>) * count, cudaMemcpyHostToDevice, st));
+	for (int pass = 0; pass < 5; ++pass)
+		for (size_t k = 0; k < lens[pass].size(); ++k) {
+			ConvGroup::List l{pass, lens[pass][k], nullptr, (int)items[pass][k].size()};
+			MM_CUDA(cudaMalloc(&l.items, sizeof(int2) * l.n));
+			MM_CUDA(cudaMemcpyAsync(l.items, items[pass][k].data(), sizeof(int2) * l.n, cudaMemcpyHostToDevice, st));
+			g->lists.push_back(l);
+			MM_TRY(group_smem<T>(pass, l.len));
+		}
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+} // namespace
+
+mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int count, cudaStream_t st)
+{
+	if (!out || !members || count < 1) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: no members");
+	ConvGroup *g = new ConvGroup();
+	g->prec = members[0].plan ? members[0].plan->prec : MM_F32;
+	g->count = count;
+	const mm_status r = g->prec == MM_F64 ? group_create<double>(g, members, count, st)
+	                                       : group_create<float>(g, members, count, st);
+	if (r != MM_OK) {
+		delete g;
+		return r;
+	}
+	*out = g;
+	return MM_OK;
+}
+
+mm_status conv_group_execute(ConvGroup *g, int input, const int *active_device, cudaStream_t st)
+{
+	if (!g || input < 0 || input > 2) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad input selector");
+	for (const auto &l : g->lists) {
+		if (g->prec == MM_F64) group_launch<double>(g, l, input, active_device, st);
+		else group_launch<float>(g, l, input, active_device, st);
+		MM_TRY(after_launch("k_conv_grp"));
+	}
+	return MM_OK;
+}
+
+int conv_group_launches(const ConvGroup *g) { return g ? (int)g->lists.size() : 0; }
+
+void conv_group_destroy(ConvGroup *g) { delete g; }
 
 } // namespace mm
 

@@ -61,6 +61,23 @@ mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const
 // Number of kernel launches one conv_execute issues.
 int conv_launches(const ConvPlan *p);
 
+// Grouped convolution over many plans of the same precision, each with power-of-two 3-D padding
+// and a register z pass: one launch per pass and transform length covers every member.  M[k]
+// are up to three candidate inputs per member (selected per call), H its output; members whose
+// active flag (device int per member, optional) is 0 are skipped.
+struct ConvGroup;
+struct ConvGroupMember {
+	ConvPlan *plan;
+	const void *M[3];
+	void *H;
+	const uint8_t *reg;
+	const void *ms_tab;  // 256 entries
+};
+mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int count, cudaStream_t st);
+mm_status conv_group_execute(ConvGroup *g, int input, const int *active_device, cudaStream_t st);
+int conv_group_launches(const ConvGroup *g);
+void conv_group_destroy(ConvGroup *g);
+
 FftRadices fft_factor(int n);
 
 } // namespace mm

@@ -306,6 +306,57 @@ MM_API mm_status mm_solver_relax(mm_solver *s, int criterion, double threshold, 
 /* <M> [A/m] averaged over all cells (VectorMatrix::average). Synchronises `stream`. */
 MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg_host3, void *stream);
 
+/* ---------------------------------------------------------------------------------------------
+ * Batched relaxations (no reference counterpart: the reference relaxes one world at a time).
+ * Many independent instances of uneven size advance in lock step, one Runge-Kutta attempt per
+ * round for every instance still running, as grouped launches (one per pass and transform length
+ * for the demag convolution, one per stage for the fused stage kernel) replayed from CUDA graphs;
+ * step control, the accept step and the stop test run on the device per instance.
+ * Each instance: a box of nx*ny*nz cells with a material mask (1: material with Ms, A, alpha;
+ * 0: empty), demag + exchange + LLG, dp54 with the reference's step-size controller, power-of-two
+ * padding (a single layer is padded to 2 in z).  An instance stops at the first accepted step
+ * whose step count is a multiple of check_every_nth_step and whose state has
+ * max |m x H_eff| / Ms < max_torque (H_eff evaluated at the accepted state).
+ * ------------------------------------------------------------------------------------------- */
+typedef struct {
+	int nx, ny, nz;
+	double dx, dy, dz;
+	double Ms, A, alpha;
+} mm_batch_instance;
+
+typedef struct {
+	int precision;            /* MM_F32 (compensated state) or MM_F64 */
+	double eps_abs, eps_rel;  /* MicroMagneticsStepSizeController tolerances */
+	double h0;                /* first step size */
+	double max_torque;        /* stop threshold of max |m x H_eff| / Ms */
+	int check_every_nth_step;
+} mm_batch_config;
+
+typedef struct {
+	int status;               /* 0 running, 1 relaxed, 2 stopped on a non-finite state */
+	int steps, attempts, rejected;
+	double t, h;
+} mm_batch_result;
+
+typedef struct mm_batch mm_batch;
+
+/* masks_host: the instances' masks back to back (N_i bytes each, 0/1), NULL = all material. */
+MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *config, int count,
+                                 const mm_batch_instance *instances_host, const uint8_t *masks_host,
+                                 void *stream);
+MM_API mm_status mm_batch_destroy(mm_batch *b);
+/* M of instance `index` (FP64 device array, A/m, normalised to Ms); the next relaxation starts
+ * from t = 0 with step size h0 for every instance. */
+MM_API mm_status mm_batch_set_M(mm_batch *b, int index, const double *M_device, void *stream);
+MM_API mm_status mm_batch_get_M(mm_batch *b, int index, double *M_device, void *stream);
+/* Runs at most max_rounds rounds, checking every check_interval rounds (one small device-to-host
+ * copy) whether any instance still runs.  *rounds_out: rounds run.  Synchronises `stream`. */
+MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_interval,
+                                long long *rounds_out, void *stream);
+MM_API mm_status mm_batch_results(mm_batch *b, mm_batch_result *results_host, void *stream);
+/* Kernel launches in one captured round (the first round evaluates k_0, later ones do not). */
+MM_API mm_status mm_batch_launches_per_round(mm_batch *b, int *first, int *later);
+
 #ifdef __cplusplus
 }
 #endif

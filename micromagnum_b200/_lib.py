@@ -53,6 +53,28 @@ class mm_solver_config(ctypes.Structure):
     ]
 
 
+class mm_batch_instance(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
+        ("Ms", ctypes.c_double), ("A", ctypes.c_double), ("alpha", ctypes.c_double),
+    ]
+
+
+class mm_batch_config(ctypes.Structure):
+    _fields_ = [
+        ("precision", ctypes.c_int), ("eps_abs", ctypes.c_double), ("eps_rel", ctypes.c_double),
+        ("h0", ctypes.c_double), ("max_torque", ctypes.c_double), ("check_every_nth_step", ctypes.c_int),
+    ]
+
+
+class mm_batch_result(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int), ("steps", ctypes.c_int), ("attempts", ctypes.c_int), ("rejected", ctypes.c_int),
+        ("t", ctypes.c_double), ("h", ctypes.c_double),
+    ]
+
+
 class mm_solver_stats(ctypes.Structure):
     _fields_ = [
         ("t", ctypes.c_double), ("h", ctypes.c_double), ("h_next", ctypes.c_double),
@@ -102,6 +124,14 @@ _PROTOS = [
     ("mm_solver_stats_get", _I, [_VP, ctypes.POINTER(mm_solver_stats), _VP]),
     ("mm_solver_average_M", _I, [_VP, _DP, _VP]),
     ("mm_solver_relax_norms", _I, [_VP, _DP, _VP]),
+    ("mm_batch_create", _I, [ctypes.POINTER(_VP), ctypes.POINTER(mm_batch_config), _I,
+                             ctypes.POINTER(mm_batch_instance), _VP, _VP]),
+    ("mm_batch_destroy", _I, [_VP]),
+    ("mm_batch_set_M", _I, [_VP, _I, _VP, _VP]),
+    ("mm_batch_get_M", _I, [_VP, _I, _VP, _VP]),
+    ("mm_batch_relax", _I, [_VP, ctypes.c_longlong, _I, ctypes.POINTER(ctypes.c_longlong), _VP]),
+    ("mm_batch_results", _I, [_VP, ctypes.POINTER(mm_batch_result), _VP]),
+    ("mm_batch_launches_per_round", _I, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("mm_solver_relax", _I, [_VP, _I, _D, _I, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int), _DP, _VP]),
 ]
 

@@ -53,6 +53,7 @@ struct DevState {
 	int accept;
 	int not_finite;
 	int pad[2];
+	double max_tq2;   // max (|m x H_eff| / Ms)^2 at the last stage's input (batched relaxations)
 };
 
 constexpr int MAXS = 8;
@@ -283,6 +284,95 @@ constexpr int STAGE_CPT = 2;
 template <typename T>
 constexpr int stage_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }  // FP64 needs ~126 registers
 
+// One tile (32*STAGE_CPT x 8 cells of plane z) of the fused stage; the maxima of the error, of
+// |k_0| and (TORQUE) of |m x H_eff| / Ms accumulate in e2, k02, tq2.
+template <typename T, bool COMP, int S, bool TORQUE>
+__device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__restrict__ msr, const StageCoef &sc,
+                                           const T *__restrict__ y_in, const T *__restrict__ Hd,
+                                           const T *__restrict__ yhi, const T *__restrict__ ylo, T *const *K,
+                                           T *__restrict__ y_out, T *__restrict__ y_out_lo,
+                                           const DevState *__restrict__ st, int tile, int tiles_x, int tiles_y,
+                                           T &e2, T &k02, T &tq2)
+{
+	const size_t n = (size_t)a.nx * a.ny * a.nz;
+	const double h = st->h;
+	const int tx = tile % tiles_x, rest = tile / tiles_x;
+	const int yy = (rest % tiles_y) * blockDim.y + threadIdx.y;
+	const int z = rest / tiles_y;
+	const double t = st->t + sc.a_i * h;
+	V3<T> ki[STAGE_CPT];
+	size_t idx[STAGE_CPT];
+	bool in[STAGE_CPT];
+#pragma unroll
+	for (int u = 0; u < STAGE_CPT; ++u) {
+		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
+		in[u] = x < a.nx && yy < a.ny;
+		idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
+		if (in[u]) {
+			V3<T> Heff;
+			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
+			cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
+			if (TORQUE) {
+				const T ms = mat_of(a, idx[u]).Ms;
+				if (ms != T(0)) {
+					const V3<T> c = cross(load3(y_in, idx[u], n), Heff);
+					tq2 = nan_max(tq2, dot(c, c) / (ms * ms));
+				}
+			}
+		}
+	}
+#pragma unroll
+	for (int u = 0; u < STAGE_CPT; ++u) {
+		if (!in[u]) continue;
+		const size_t i = idx[u];
+		if (!sc.last) {
+			if (sc.write_next) {
+				V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
+#pragma unroll
+				for (int l = 0; l < S; ++l) {
+					const T f = (T)(h * sc.bn[l]);
+					if (f != T(0)) acc = acc + f * load3(K[l], i, n);
+				}
+				acc = acc + (T)(h * sc.bn[S]) * ki[u];
+				if (COMP) acc = load3(yhi, i, n) + acc;
+				store3(y_out, i, n, acc);
+			}
+			if (sc.reduce_k0) {
+				const V3<T> k0 = S == 0 ? ki[u] : load3(K[0], i, n);
+				k02 = max(k02, dot(k0, k0));
+			}
+		} else {
+			V3<T> err = v3<T>(0, 0, 0);
+			V3<T> acc = v3<T>(0, 0, 0);
+#pragma unroll
+			for (int l = 0; l <= S; ++l) {
+				const T fe = (T)(h * sc.ec[l]);
+				const T fc = (T)(h * sc.bn[l]);
+				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
+				const V3<T> kl = l == S ? ki[u] : load3(K[l], i, n);
+				err = err + fe * kl;
+				if (sc.write_new) acc = acc + fc * kl;
+			}
+			e2 = nan_max(e2, dot(err, err));
+			if (sc.write_new) {
+				if (COMP) {
+					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
+					const V3<T> hi = load3(yhi, i, n);
+					const V3<T> d = load3(ylo, i, n) + acc;
+					const V3<T> s = hi + d;
+					const V3<T> bb = s - hi;
+					const V3<T> lo = (hi - (s - bb)) + (d - bb);
+					store3(y_out, i, n, s);
+					store3(y_out_lo, i, n, lo);
+				} else {
+					store3(y_out, i, n, load3(yhi, i, n) + acc);
+				}
+			}
+		}
+		store3(K[S], i, n, ki[u]);
+	}
+}
+
 template <typename T, bool COMP, int S>
 __global__ void __launch_bounds__(256, stage_min_blocks<T>())
     k_stage(CellArgs<T> a, StageCoef sc, const T *__restrict__ y_in, const T *__restrict__ Hd,
@@ -292,91 +382,21 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 {
 	__shared__ T msr[256];
 	load_ms_table(a, msr);
-	const size_t n = (size_t)a.nx * a.ny * a.nz;
-	const double h = st->h;
-	const double t = st->t + sc.a_i * h;
 	T *const *K = ktab->k;
-	T e2 = T(0), k02 = T(0);
-	for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-		const int tx = tile % tiles_x, rest = tile / tiles_x;
-		const int yy = (rest % tiles_y) * blockDim.y + threadIdx.y;
-		const int z = rest / tiles_y;
-		V3<T> ki[STAGE_CPT];
-		size_t idx[STAGE_CPT];
-		bool in[STAGE_CPT];
-#pragma unroll
-		for (int u = 0; u < STAGE_CPT; ++u) {
-			const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
-			in[u] = x < a.nx && yy < a.ny;
-			idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
-			if (in[u]) {
-				V3<T> Heff;
-				const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
-				cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
-			}
-		}
-#pragma unroll
-		for (int u = 0; u < STAGE_CPT; ++u) {
-			if (!in[u]) continue;
-			const size_t i = idx[u];
-			if (!sc.last) {
-				if (sc.write_next) {
-					V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
-#pragma unroll
-					for (int l = 0; l < S; ++l) {
-						const T f = (T)(h * sc.bn[l]);
-						if (f != T(0)) acc = acc + f * load3(K[l], i, n);
-					}
-					acc = acc + (T)(h * sc.bn[S]) * ki[u];
-					if (COMP) acc = load3(yhi, i, n) + acc;
-					store3(y_out, i, n, acc);
-				}
-				if (sc.reduce_k0) {
-					const V3<T> k0 = S == 0 ? ki[u] : load3(K[0], i, n);
-					k02 = max(k02, dot(k0, k0));
-				}
-			} else {
-				V3<T> err = v3<T>(0, 0, 0);
-				V3<T> acc = v3<T>(0, 0, 0);
-#pragma unroll
-				for (int l = 0; l <= S; ++l) {
-					const T fe = (T)(h * sc.ec[l]);
-					const T fc = (T)(h * sc.bn[l]);
-					if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
-					const V3<T> kl = l == S ? ki[u] : load3(K[l], i, n);
-					err = err + fe * kl;
-					if (sc.write_new) acc = acc + fc * kl;
-				}
-				e2 = nan_max(e2, dot(err, err));
-				if (sc.write_new) {
-					if (COMP) {
-						// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
-						const V3<T> hi = load3(yhi, i, n);
-						const V3<T> d = load3(ylo, i, n) + acc;
-						const V3<T> s = hi + d;
-						const V3<T> bb = s - hi;
-						const V3<T> lo = (hi - (s - bb)) + (d - bb);
-						store3(y_out, i, n, s);
-						store3(y_out_lo, i, n, lo);
-					} else {
-						store3(y_out, i, n, load3(yhi, i, n) + acc);
-					}
-				}
-			}
-			store3(K[S], i, n, ki[u]);
-		}
-	}
+	T e2 = T(0), k02 = T(0), tq2 = T(0);
+	for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+		stage_tile<T, COMP, S, false>(a, msr, sc, y_in, Hd, yhi, ylo, K, y_out, y_out_lo, st, tile, tiles_x, tiles_y,
+		                              e2, k02, tq2);
 	if (sc.last) block_max_to(red_err, e2);
 	if (sc.reduce_k0) block_max_to(red_k0, k02);
 }
 
 // Accepted step: m <- y_{n+1} / |y_{n+1}| (VectorMatrix::normalize to Ms, in unit form).
 template <typename T, bool COMP>
-__global__ void __launch_bounds__(256) k_accept(size_t n, const T *__restrict__ ynew,
-                                                const T *__restrict__ ynew_lo, T *__restrict__ m,
-                                                T *__restrict__ m_lo)
+__device__ __forceinline__ void accept_cell(size_t n, const T *__restrict__ ynew, const T *__restrict__ ynew_lo,
+                                            T *__restrict__ m, T *__restrict__ m_lo, size_t i)
 {
-	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+	{
 		if (COMP) {
 			const double x = (double)ynew[i] + (double)ynew_lo[i];
 			const double y = (double)ynew[i + n] + (double)ynew_lo[i + n];
@@ -397,11 +417,21 @@ __global__ void __launch_bounds__(256) k_accept(size_t n, const T *__restrict__ 
 	}
 }
 
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_accept(size_t n, const T *__restrict__ ynew,
+                                                const T *__restrict__ ynew_lo, T *__restrict__ m,
+                                                T *__restrict__ m_lo)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+		accept_cell<T, COMP>(n, ynew, ynew_lo, m, m_lo, i);
+}
+
 // MicroMagneticsStepSizeController.adjust_stepsize (micro_magnetics_stepsize_controller.py:
 // 35-73), in double, on one thread; also swaps k_0 / k_last for first-same-as-last tableaus.
 template <typename T>
-__global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double eps_rel, int order,
-                             int fsal, int s, DevState *host_copy, const int *conv_timeout)
+__device__ __forceinline__ void control_attempt(DevState *st, KTab<T> *ktab, double eps_abs, double eps_rel,
+                                                int order, int fsal, int s, DevState *host_copy,
+                                                const int *conv_timeout)
 {
 	const double h = st->h;
 	const double e_abs = sqrt(st->max_err2);
@@ -428,7 +458,7 @@ __global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double
 	st->accept = accept;
 	st->h_new = h_new;
 	st->not_finite = timed_out ? 2 : !finite;
-	*host_copy = *st;
+	if (host_copy) *host_copy = *st;
 	st->max_err2 = 0.0;
 	st->max_k02 = 0.0;
 	if (fsal) {
@@ -436,6 +466,13 @@ __global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double
 		ktab->k[0] = ktab->k[s - 1];
 		ktab->k[s - 1] = t;
 	}
+}
+
+template <typename T>
+__global__ void k_controller(DevState *st, KTab<T> *ktab, double eps_abs, double eps_rel, int order,
+                             int fsal, int s, DevState *host_copy, const int *conv_timeout)
+{
+	control_attempt<T>(st, ktab, eps_abs, eps_rel, order, fsal, s, host_copy, conv_timeout);
 }
 
 // Effective field and dM/dt in A/m (FP64 outputs) at the state m.
@@ -1104,11 +1141,33 @@ mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uin
 } // namespace
 } // namespace mm
 
+namespace mm {
+namespace {
+mm_status solver_create(mm_solver **out, const mm_solver_config *config, int num_materials,
+                        const mm_material *materials_host, const uint8_t *regions_host,
+                        const double *tensor_device, void *stream, int min_pz);
+} // namespace
+} // namespace mm
+
 extern "C" {
 
 MM_API mm_status mm_solver_create(mm_solver **out, const mm_solver_config *config, int num_materials,
                                   const mm_material *materials_host, const uint8_t *regions_host,
                                   const double *tensor_device, void *stream)
+{
+	return solver_create(out, config, num_materials, materials_host, regions_host, tensor_device, stream, 1);
+}
+
+} // extern "C"
+
+namespace mm {
+namespace {
+
+// mm_solver_create with a lower bound on the padded z length (the batch pads a single layer to
+// 2 so that every instance takes the 3-D power-of-two passes).
+mm_status solver_create(mm_solver **out, const mm_solver_config *config, int num_materials,
+                        const mm_material *materials_host, const uint8_t *regions_host,
+                        const double *tensor_device, void *stream, int min_pz)
 {
 	if (!out || !config || !materials_host || num_materials <= 0 || num_materials > 256)
 		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid argument");
@@ -1130,6 +1189,7 @@ MM_API mm_status mm_solver_create(mm_solver **out, const mm_solver_config *confi
 	s->px = mm_round_tensor_dimension(c.nx, 0, c.padding);
 	s->py = mm_round_tensor_dimension(c.ny, 0, c.padding);
 	s->pz = mm_round_tensor_dimension(c.nz, 0, c.padding);
+	if (s->pz > 0 && s->pz < min_pz) s->pz = min_pz;
 	if (s->px <= 0 || s->py <= 0 || s->pz <= 0) {
 		delete s;
 		return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_create: invalid padding");
@@ -1146,6 +1206,11 @@ MM_API mm_status mm_solver_create(mm_solver **out, const mm_solver_config *confi
 	*out = s;
 	return MM_OK;
 }
+
+} // namespace
+} // namespace mm
+
+extern "C" {
 
 MM_API mm_status mm_solver_destroy(mm_solver *s)
 {
@@ -1356,6 +1421,504 @@ MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg3, void *stream)
 	if (!s || !avg3) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_average_M: null argument");
 	cudaStream_t st = as_stream(stream);
 	return s->cfg.precision == MM_F64 ? average<double>(s, avg3, st) : average<float>(s, avg3, st);
+}
+
+} // extern "C"
+
+// ================================================================================================
+// Batched relaxations: many independent instances of uneven size advance in lock step, one
+// Runge-Kutta attempt per round for every active instance.  Each instance is a full solver
+// (own state, stages, tensor and spectra); the rounds run as grouped launches (one per pass and
+// transform length for the convolution, one per stage for the fused stage kernel) over work
+// lists of (instance, tile), and the step controller, the accept step and the relaxation check
+// run on the device per instance, so a captured round needs no host decision.
+// ================================================================================================
+namespace mm {
+namespace {
+
+template <typename T>
+struct BDesc {
+	CellArgs<T> a;
+	T *m, *m_lo, *ys[2], *hd, *ynew_lo;
+	KTab<T> *kt;
+	DevState *ds;
+	int n, tiles_x, tiles_y, ntiles;
+};
+
+constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage kernel
+constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
+
+// Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
+template <typename T, bool COMP, int S, bool TORQUE>
+__global__ void __launch_bounds__(256, stage_min_blocks<T>())
+    k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items,
+                const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (!active[it.x]) return;
+	const BDesc<T> &g = d[it.x];
+	__shared__ CellArgs<T> a;
+	__shared__ T msr[256];
+	if (threadIdx.x == 0 && threadIdx.y == 0) a = g.a;
+	__syncthreads();
+	load_ms_table(a, msr);
+	const T *y_in = in == 0 ? g.m : g.ys[in - 1];
+	T *K[MAXS];
+#pragma unroll
+	for (int l = 0; l < MAXS; ++l) K[l] = g.kt->k[l];
+	T e2 = T(0), k02 = T(0), tq2 = T(0);
+	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
+		stage_tile<T, COMP, S, TORQUE>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds, it.y + k,
+		                               g.tiles_x, g.tiles_y, e2, k02, tq2);
+	if (sc.last) block_max_to(&g.ds->max_err2, e2);
+	if (sc.reduce_k0) block_max_to(&g.ds->max_k02, k02);
+	if (TORQUE) block_max_to(&g.ds->max_tq2, tq2);
+}
+
+// Grouped first-same-as-last first stage, y_1 = y_n + h b_10 k_0, into ys[0].
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_prepare1_grp(const BDesc<T> *__restrict__ d, double b10,
+                                                      const int2 *__restrict__ items, const int *__restrict__ active)
+{
+	const int2 it = items[blockIdx.x];
+	if (!active[it.x]) return;
+	const BDesc<T> &g = d[it.x];
+	const size_t n3 = 3 * (size_t)g.n;
+	const T f = (T)(g.ds->h * b10);
+	const T *k0 = g.kt->k[0];
+	const size_t end = min(n3, (size_t)(it.y + 1) * BATCH_CHUNK);
+	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x) {
+		if (COMP) g.ys[0][i] = g.m[i] + (g.m_lo[i] + f * k0[i]);
+		else g.ys[0][i] = g.m[i] + f * k0[i];
+	}
+}
+
+// Grouped accept: m <- y_{n+1}/|y_{n+1}| for the instances whose attempt the controller accepted.
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(256) k_accept_grp(const BDesc<T> *__restrict__ d, int last_buf,
+                                                    const int2 *__restrict__ items)
+{
+	const int2 it = items[blockIdx.x];
+	const BDesc<T> &g = d[it.x];
+	if (!g.ds->accept) return;
+	const size_t n = (size_t)g.n;
+	const T *ynew = g.ys[last_buf];
+	const size_t end = min(n, (size_t)(it.y + 1) * BATCH_CHUNK);
+	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x)
+		accept_cell<T, COMP>(n, ynew, g.ynew_lo, g.m, g.m_lo, i);
+}
+
+// Per-instance bookkeeping of a batch (device; copied to the host on request).
+struct BState {
+	int steps, attempts, rejected, status;  // status: 0 running, 1 relaxed, 2 non-finite state
+	double t, h;
+};
+
+// Grouped step controller (one thread per instance): the single-instance controller's decision,
+// then time and step-size update, counters, and the relaxation check on the accepted state
+// (its torque was reduced by the last stage, whose input is y_{n+1} for a first-same-as-last
+// tableau).  Finished instances leave `active`; the accept kernel still applies their last step.
+template <typename T>
+__global__ void k_controller_grp(const BDesc<T> *__restrict__ d, int count, double eps_abs, double eps_rel,
+                                 int order, int fsal, int s, double tq_thr2, int check_every, BState *bs,
+                                 int *active)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= count) return;
+	DevState *st = d[i].ds;
+	if (!active[i]) {
+		st->accept = 0;
+		return;
+	}
+	const double h = st->h;
+	const double tq2 = st->max_tq2;
+	st->max_tq2 = 0.0;
+	control_attempt<T>(st, d[i].kt, eps_abs, eps_rel, order, fsal, s, nullptr, nullptr);
+	BState &b = bs[i];
+	b.attempts++;
+	if (st->not_finite) {
+		b.status = 2;
+		active[i] = 0;
+		st->accept = 0;
+	} else if (st->accept) {
+		st->t += h;
+		st->h = st->h_new;
+		b.steps++;
+		if (check_every > 0 && b.steps % check_every == 0 && tq2 < tq_thr2) {
+			b.status = 1;
+			active[i] = 0;
+		}
+	} else {
+		st->h = st->h_new;
+		b.rejected++;
+	}
+	b.t = st->t;
+	b.h = st->h;
+}
+
+// Resets time, step size, counters and reductions of every instance (start of a relaxation).
+__global__ void k_batch_reset(DevState *const *ds, int count, double h0, BState *bs, int *active)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if (i >= count) return;
+	DevState *st = ds[i];
+	st->t = 0.0;
+	st->h = h0;
+	st->max_err2 = st->max_k02 = st->max_tq2 = 0.0;
+	st->accept = 0;
+	st->not_finite = 0;
+	bs[i] = BState{0, 0, 0, 0, 0.0, h0};
+	active[i] = 1;
+}
+
+} // namespace
+} // namespace mm
+
+struct mm_batch {
+	int count = 0;
+	int prec = MM_F32;
+	mm_batch_config cfg{};
+	std::vector<mm_solver *> inst;
+	mm::ConvGroup *conv = nullptr;
+	void *desc = nullptr;                         // BDesc<T>[count]
+	mm::DevState **ds_list = nullptr;             // device array of the instances' DevState pointers
+	int2 *stage_items = nullptr, *cell3_items = nullptr, *cell_items = nullptr;
+	int n_stage = 0, n_cell3 = 0, n_cell = 0;
+	int *active = nullptr;
+	mm::BState *bs = nullptr;
+	mm::BState *bs_h = nullptr;                   // pinned
+	int *active_h = nullptr;                      // pinned
+	bool need_first = true;                       // next round evaluates k_0 (after a reset)
+	cudaStream_t gs = nullptr;
+	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // [0] first round (k_0 evaluated), [1] later rounds
+	int launches_per_round[2] = {0, 0};
+};
+
+namespace mm {
+namespace {
+
+void free_batch(mm_batch *b)
+{
+	if (!b) return;
+	for (auto &g : b->gexec)
+		if (g) cudaGraphExecDestroy(g);
+	if (b->gs) cudaStreamDestroy(b->gs);
+	if (b->ev_in) cudaEventDestroy(b->ev_in);
+	if (b->ev_out) cudaEventDestroy(b->ev_out);
+	conv_group_destroy(b->conv);
+	cudaFree(b->desc);
+	cudaFree(b->ds_list);
+	cudaFree(b->stage_items);
+	cudaFree(b->cell3_items);
+	cudaFree(b->cell_items);
+	cudaFree(b->active);
+	cudaFree(b->bs);
+	cudaFreeHost(b->bs_h);
+	cudaFreeHost(b->active_h);
+	for (mm_solver *s : b->inst) free_solver(s);
+	delete b;
+}
+
+template <typename T, bool COMP, int S>
+void launch_stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, cudaStream_t st)
+{
+	const BDesc<T> *d = (const BDesc<T> *)b->desc;
+	if (sc.last)
+		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items, b->active);
+	else
+		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items, b->active);
+}
+
+template <typename T, bool COMP>
+mm_status stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, cudaStream_t st)
+{
+	switch (sc.stage) {
+	case 0: launch_stage_grp<T, COMP, 0>(b, sc, in, out, st); break;
+	case 1: launch_stage_grp<T, COMP, 1>(b, sc, in, out, st); break;
+	case 2: launch_stage_grp<T, COMP, 2>(b, sc, in, out, st); break;
+	case 3: launch_stage_grp<T, COMP, 3>(b, sc, in, out, st); break;
+	case 4: launch_stage_grp<T, COMP, 4>(b, sc, in, out, st); break;
+	case 5: launch_stage_grp<T, COMP, 5>(b, sc, in, out, st); break;
+	case 6: launch_stage_grp<T, COMP, 6>(b, sc, in, out, st); break;
+	default: return fail(MM_ERR_UNSUPPORTED, "batch: stage index beyond the dp54 tableau");
+	}
+	return after_launch("k_stage_grp");
+}
+
+// One lock-step round: an attempt of every active instance, its controller decision and the
+// accept step.  first: k_0 is evaluated at the state (start of a relaxation); otherwise it is the
+// previous attempt's last stage (first same as last, also after a rejection, like the reference).
+template <typename T>
+mm_status batch_round(mm_batch *b, bool first, cudaStream_t st)
+{
+	constexpr bool COMP = sizeof(T) == 4;
+	const Tableau &tb = b->inst[0]->tab;
+	if (first) {
+		StageCoef sc{};
+		sc.stage = 0;
+		sc.a_i = tb.a[0];
+		sc.write_next = 1;
+		sc.bn[0] = tb.b[1][0];
+		MM_TRY(conv_group_execute(b->conv, 0, b->active, st));
+		MM_TRY((stage_grp<T, COMP>(b, sc, 0, 0, st)));
+	} else {
+		k_prepare1_grp<T, COMP><<<b->n_cell3, 256, 0, st>>>((const BDesc<T> *)b->desc, tb.b[1][0], b->cell3_items,
+		                                                   b->active);
+		MM_TRY(after_launch("k_prepare1_grp"));
+	}
+	int last_buf = 0;
+	for (int i = 1; i < tb.s; ++i) {
+		StageCoef sc{};
+		sc.stage = i;
+		sc.last = (i == tb.s - 1);
+		sc.a_i = tb.a[i];
+		sc.reduce_k0 = (i == 1);
+		if (!sc.last) {
+			sc.write_next = 1;
+			for (int l = 0; l <= i; ++l) sc.bn[l] = tb.b[i + 1][l];
+		} else {
+			sc.write_new = COMP || !tb.fsal;
+			for (int l = 0; l <= i; ++l) {
+				sc.bn[l] = tb.c[l];
+				sc.ec[l] = tb.ec[l];
+			}
+		}
+		const int in = 1 + ((i - 1) & 1);
+		MM_TRY(conv_group_execute(b->conv, in, b->active, st));
+		MM_TRY((stage_grp<T, COMP>(b, sc, in, i & 1, st)));
+		if (sc.last) last_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
+	}
+	const double thr = b->cfg.max_torque;
+	k_controller_grp<T><<<(b->count + 127) / 128, 128, 0, st>>>(
+	    (const BDesc<T> *)b->desc, b->count, b->cfg.eps_abs, b->cfg.eps_rel, tb.order, tb.fsal, tb.s, thr * thr,
+	    b->cfg.check_every_nth_step, b->bs, b->active);
+	MM_TRY(after_launch("k_controller_grp"));
+	k_accept_grp<T, COMP><<<b->n_cell, 256, 0, st>>>((const BDesc<T> *)b->desc, last_buf, b->cell_items);
+	MM_TRY(after_launch("k_accept_grp"));
+	return MM_OK;
+}
+
+// Captures one round (first or later) into a graph on the batch's private stream.
+template <typename T>
+mm_status batch_graph(mm_batch *b, int v)
+{
+	cudaGraph_t g = nullptr;
+	const uint64_t l0 = launch_counter().load();
+	MM_CUDA(cudaStreamBeginCapture(b->gs, cudaStreamCaptureModeThreadLocal));
+	const mm_status r = batch_round<T>(b, v == 0, b->gs);
+	const cudaError_t e = cudaStreamEndCapture(b->gs, &g);
+	if (r != MM_OK) {
+		if (g) cudaGraphDestroy(g);
+		return r;
+	}
+	MM_CUDA(e);
+	const cudaError_t ei = cudaGraphInstantiate(&b->gexec[v], g, 0);
+	cudaGraphDestroy(g);
+	MM_CUDA(ei);
+	b->launches_per_round[v] = (int)(launch_counter().load() - l0);
+	launch_counter().fetch_sub(b->launches_per_round[v]);  // counted again at each replay
+	return MM_OK;
+}
+
+template <typename T>
+mm_status batch_setup(mm_batch *b, cudaStream_t st)
+{
+	std::vector<BDesc<T>> h(b->count);
+	std::vector<ConvGroupMember> mem(b->count);
+	std::vector<DevState *> dsl(b->count);
+	std::vector<int2> si, c3, c1;
+	for (int i = 0; i < b->count; ++i) {
+		mm_solver *s = b->inst[i];
+		BDesc<T> &d = h[i];
+		d.a = args_of<T>(s);
+		d.m = (T *)s->m;
+		d.m_lo = (T *)s->m_lo;
+		d.ys[0] = (T *)s->ys[0];
+		d.ys[1] = (T *)s->ys[1];
+		d.hd = (T *)s->hd;
+		d.ynew_lo = (T *)s->ynew_lo;
+		d.kt = (KTab<T> *)s->ktab;
+		d.ds = s->dst;
+		d.n = (int)s->n;
+		const dim3 tg = stage_grid(s->cfg);
+		d.tiles_x = (int)tg.x;
+		d.tiles_y = (int)tg.y;
+		d.ntiles = (int)(tg.x * tg.y * tg.z);
+		for (int t = 0; t < d.ntiles; t += BATCH_TILES) si.push_back(make_int2(i, t));
+		for (int c = 0; c * (size_t)BATCH_CHUNK < 3 * s->n; ++c) c3.push_back(make_int2(i, c));
+		for (int c = 0; c * (size_t)BATCH_CHUNK < s->n; ++c) c1.push_back(make_int2(i, c));
+		mem[i] = ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1]}, s->hd, s->reg, s->ms_tab};
+		dsl[i] = s->dst;
+	}
+	MM_TRY(conv_group_create(&b->conv, mem.data(), b->count, st));
+	auto up = [&](void **dst, const void *src, size_t bytes) -> mm_status {
+		MM_CUDA(cudaMalloc(dst, bytes));
+		MM_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st));
+		return MM_OK;
+	};
+	MM_TRY(up(&b->desc, h.data(), sizeof(BDesc<T>) * b->count));
+	MM_TRY(up((void **)&b->ds_list, dsl.data(), sizeof(DevState *) * b->count));
+	MM_TRY(up((void **)&b->stage_items, si.data(), sizeof(int2) * si.size()));
+	MM_TRY(up((void **)&b->cell3_items, c3.data(), sizeof(int2) * c3.size()));
+	MM_TRY(up((void **)&b->cell_items, c1.data(), sizeof(int2) * c1.size()));
+	b->n_stage = (int)si.size();
+	b->n_cell3 = (int)c3.size();
+	b->n_cell = (int)c1.size();
+	MM_CUDA(cudaMalloc(&b->active, sizeof(int) * b->count));
+	MM_CUDA(cudaMalloc(&b->bs, sizeof(BState) * b->count));
+	MM_CUDA(cudaMallocHost(&b->bs_h, sizeof(BState) * b->count));
+	MM_CUDA(cudaMallocHost(&b->active_h, sizeof(int) * b->count));
+	MM_CUDA(cudaStreamCreateWithFlags(&b->gs, cudaStreamNonBlocking));
+	MM_CUDA(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
+	MM_CUDA(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
+	k_batch_reset<<<(b->count + 127) / 128, 128, 0, st>>>(b->ds_list, b->count, b->cfg.h0, b->bs, b->active);
+	MM_TRY(after_launch("k_batch_reset"));
+	MM_CUDA(cudaStreamSynchronize(st));
+	MM_TRY(batch_graph<T>(b, 0));
+	MM_TRY(batch_graph<T>(b, 1));
+	return MM_OK;
+}
+
+} // namespace
+} // namespace mm
+
+extern "C" {
+
+MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *cfg, int count,
+                                 const mm_batch_instance *inst_host, const uint8_t *masks_host, void *stream)
+{
+	if (!out || !cfg || count < 1 || !inst_host) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid argument");
+	if (cfg->precision != MM_F64 && cfg->precision != MM_F32)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid precision");
+	if (!(cfg->eps_abs > 0) || !(cfg->eps_rel > 0) || !(cfg->h0 > 0) || !(cfg->max_torque >= 0) ||
+	    cfg->check_every_nth_step < 1)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid tolerances, h0, torque or check interval");
+	cudaStream_t st = as_stream(stream);
+	mm_batch *b = new mm_batch();
+	b->count = count;
+	b->prec = cfg->precision;
+	b->cfg = *cfg;
+	size_t off = 0;
+	for (int i = 0; i < count && true; ++i) {
+		const mm_batch_instance &q = inst_host[i];
+		mm_solver_config c{};
+		c.nx = q.nx; c.ny = q.ny; c.nz = q.nz;
+		c.dx = q.dx; c.dy = q.dy; c.dz = q.dz;
+		c.precision = cfg->precision;
+		c.tableau = MM_RK_DP54;
+		c.terms = MM_TERM_DEMAG | MM_TERM_EXCHANGE;
+		c.do_precess = 1;
+		c.zl_do_precess = 1;
+		c.padding = MM_PADDING_ROUND_POT;
+		c.eps_abs = cfg->eps_abs;
+		c.eps_rel = cfg->eps_rel;
+		c.h0 = cfg->h0;
+		c.fsal_reuse_after_reject = 1;
+		mm_material mats[2] = {};
+		mats[1].Ms = q.Ms;
+		mats[1].A = q.A;
+		mats[1].alpha = q.alpha;
+		mats[0].alpha = q.alpha;
+		const size_t n = (size_t)q.nx * q.ny * q.nz;
+		std::vector<uint8_t> ones;
+		const uint8_t *reg = masks_host ? masks_host + off : nullptr;
+		if (!reg) {
+			ones.assign(n, 1);
+			reg = ones.data();
+		}
+		off += n;
+		mm_solver *s = nullptr;
+		const mm_status r = solver_create(&s, &c, 2, mats, reg, nullptr, stream, 2);
+		if (r != MM_OK) {
+			free_batch(b);
+			return r;
+		}
+		b->inst.push_back(s);
+	}
+	const mm_status r = b->prec == MM_F64 ? batch_setup<double>(b, st) : batch_setup<float>(b, st);
+	if (r != MM_OK) {
+		free_batch(b);
+		return r;
+	}
+	*out = b;
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_destroy(mm_batch *b)
+{
+	free_batch(b);
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_set_M(mm_batch *b, int index, const double *M_device, void *stream)
+{
+	if (!b || index < 0 || index >= b->count || !M_device)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_set_M: invalid argument");
+	MM_TRY(mm_solver_set_M(b->inst[index], M_device, stream));
+	b->need_first = true;
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_get_M(mm_batch *b, int index, double *M_device, void *stream)
+{
+	if (!b || index < 0 || index >= b->count || !M_device)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_get_M: invalid argument");
+	return mm_solver_get_M(b->inst[index], M_device, stream);
+}
+
+MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_interval, long long *rounds_out,
+                                void *stream)
+{
+	if (!b || max_rounds < 0 || check_interval < 1) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_relax: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	if (b->need_first) {
+		k_batch_reset<<<(b->count + 127) / 128, 128, 0, st>>>(b->ds_list, b->count, b->cfg.h0, b->bs, b->active);
+		MM_TRY(after_launch("k_batch_reset"));
+	}
+	MM_CUDA(cudaEventRecord(b->ev_in, st));
+	MM_CUDA(cudaStreamWaitEvent(b->gs, b->ev_in, 0));
+	long long done = 0;
+	while (done < max_rounds) {
+		const int v = b->need_first ? 0 : 1;
+		MM_CUDA(cudaGraphLaunch(b->gexec[v], b->gs));
+		launch_counter().fetch_add(b->launches_per_round[v]);
+		b->need_first = false;
+		++done;
+		if (done % check_interval == 0 || done == max_rounds) {
+			MM_CUDA(cudaMemcpyAsync(b->active_h, b->active, sizeof(int) * b->count, cudaMemcpyDeviceToHost, b->gs));
+			MM_CUDA(cudaStreamSynchronize(b->gs));
+			int left = 0;
+			for (int i = 0; i < b->count; ++i) left += b->active_h[i];
+			if (!left) break;
+		}
+	}
+	MM_CUDA(cudaEventRecord(b->ev_out, b->gs));
+	MM_CUDA(cudaStreamWaitEvent(st, b->ev_out, 0));
+	MM_CUDA(cudaStreamSynchronize(st));
+	if (rounds_out) *rounds_out = done;
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_results(mm_batch *b, mm_batch_result *out_host, void *stream)
+{
+	if (!b || !out_host) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_results: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	MM_CUDA(cudaMemcpyAsync(b->bs_h, b->bs, sizeof(BState) * b->count, cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	for (int i = 0; i < b->count; ++i) {
+		const BState &s = b->bs_h[i];
+		out_host[i] = mm_batch_result{s.status, s.steps, s.attempts, s.rejected, s.t, s.h};
+	}
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_launches_per_round(mm_batch *b, int *first, int *later)
+{
+	if (!b) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_launches_per_round: null batch");
+	if (first) *first = b->launches_per_round[0];
+	if (later) *later = b->launches_per_round[1];
+	return MM_OK;
 }
 
 } // extern "C"

@@ -307,21 +307,28 @@ MM_API mm_status mm_solver_relax(mm_solver *s, int criterion, double threshold, 
 MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg_host3, void *stream);
 
 /* ---------------------------------------------------------------------------------------------
- * Batched relaxations (no reference counterpart: the reference relaxes one world at a time).
+ * Batched solves (no reference counterpart: the reference runs one world at a time).
  * Many independent instances of uneven size advance in lock step, one Runge-Kutta attempt per
- * round for every instance still running, as grouped launches (one per pass and transform length
- * for the demag convolution, one per stage for the fused stage kernel) replayed from CUDA graphs;
- * step control, the accept step and the stop test run on the device per instance.
+ * round for every running instance, as grouped launches (one per pass and transform length for
+ * the demag convolution, one per stage for the fused stage kernel) replayed from CUDA graphs; step
+ * control, the accept step and the stop test run on the device per instance.  Instances occupy
+ * slots; they can be added and removed between rounds (the rounds are rebuilt on the next call).
  * Each instance: a box of nx*ny*nz cells with a material mask (1: material with Ms, A, alpha;
- * 0: empty), demag + exchange + LLG, dp54 with the reference's step-size controller, power-of-two
- * padding (a single layer is padded to 2 in z).  An instance stops at the first accepted step
- * whose step count is a multiple of check_every_nth_step and whose state has
+ * 0: empty), demag + exchange + LLG (+ Zeeman: H_ext + H_pulse ramped linearly over pulse_rise,
+ * the reference's AlternatingField/HomogeneousField ramp), dp54 with the reference's step-size
+ * controller, power-of-two padding (a single layer is padded to 2 in z).  Stop test: t_end > 0
+ * stops at t = t_end (the step that would pass it is clamped onto it); t_end = 0 stops at the
+ * first accepted step whose step count is a multiple of check_every_nth_step and whose state has
  * max |m x H_eff| / Ms < max_torque (H_eff evaluated at the accepted state).
  * ------------------------------------------------------------------------------------------- */
 typedef struct {
 	int nx, ny, nz;
 	double dx, dy, dz;
 	double Ms, A, alpha;
+	double H_ext[3];      /* A/m */
+	double H_pulse[3];    /* A/m, reached after pulse_rise seconds */
+	double pulse_rise;
+	double t_end;         /* 0: relax (torque test) */
 } mm_batch_instance;
 
 typedef struct {
@@ -333,28 +340,40 @@ typedef struct {
 } mm_batch_config;
 
 typedef struct {
-	int status;               /* 0 running, 1 relaxed, 2 stopped on a non-finite state */
+	int status;               /* -1 free slot, 0 running (or not started), 1 finished, 2 non-finite state */
 	int steps, attempts, rejected;
 	double t, h;
 } mm_batch_result;
 
 typedef struct mm_batch mm_batch;
 
-/* masks_host: the instances' masks back to back (N_i bytes each, 0/1), NULL = all material. */
+/* Device bytes one instance keeps resident and the extra transient peak of its set-up. */
+MM_API mm_status mm_batch_instance_bytes(const mm_batch_instance *instance, int precision,
+                                         size_t *resident, size_t *transient);
+/* count instances in slots 0..count-1 (count may be 0); masks_host: their masks back to back
+ * (N_i bytes each, 0/1), NULL = all material.  An instance runs once it has a state (set_M). */
 MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *config, int count,
                                  const mm_batch_instance *instances_host, const uint8_t *masks_host,
                                  void *stream);
 MM_API mm_status mm_batch_destroy(mm_batch *b);
-/* M of instance `index` (FP64 device array, A/m, normalised to Ms); the next relaxation starts
- * from t = 0 with step size h0 for every instance. */
-MM_API mm_status mm_batch_set_M(mm_batch *b, int index, const double *M_device, void *stream);
-MM_API mm_status mm_batch_get_M(mm_batch *b, int index, double *M_device, void *stream);
-/* Runs at most max_rounds rounds, checking every check_interval rounds (one small device-to-host
- * copy) whether any instance still runs.  *rounds_out: rounds run.  Synchronises `stream`. */
+/* A new instance in a free slot (*slot_out); its tensor and spectra are built on `stream`, which
+ * may run while rounds of the other instances are on the device. */
+MM_API mm_status mm_batch_add(mm_batch *b, const mm_batch_instance *instance, const uint8_t *mask_host,
+                              int *slot_out, void *stream);
+MM_API mm_status mm_batch_remove(mm_batch *b, int slot);
+MM_API int mm_batch_slot_count(mm_batch *b);
+/* M of the instance in `slot` (FP64 device array, A/m, normalised to Ms); it (re)starts at t = 0
+ * with step size h0 in the next round. */
+MM_API mm_status mm_batch_set_M(mm_batch *b, int slot, const double *M_device, void *stream);
+MM_API mm_status mm_batch_get_M(mm_batch *b, int slot, double *M_device, void *stream);
+MM_API mm_status mm_batch_stop(mm_batch *b, int slot, void *stream);
+/* Runs at most max_rounds rounds, checking every check_interval rounds (small device-to-host
+ * copies) whether any instance still runs.  *rounds_out: rounds run.  Synchronises `stream`. */
 MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_interval,
                                 long long *rounds_out, void *stream);
+/* One result per slot (mm_batch_slot_count entries). */
 MM_API mm_status mm_batch_results(mm_batch *b, mm_batch_result *results_host, void *stream);
-/* Kernel launches in one captured round (the first round evaluates k_0, later ones do not). */
+/* Kernel launches in one captured round (with and without k_0 evaluations). */
 MM_API mm_status mm_batch_launches_per_round(mm_batch *b, int *first, int *later);
 
 #ifdef __cplusplus

@@ -58,6 +58,8 @@ class mm_batch_instance(ctypes.Structure):
         ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
         ("dx", ctypes.c_double), ("dy", ctypes.c_double), ("dz", ctypes.c_double),
         ("Ms", ctypes.c_double), ("A", ctypes.c_double), ("alpha", ctypes.c_double),
+        ("H_ext", ctypes.c_double * 3), ("H_pulse", ctypes.c_double * 3), ("pulse_rise", ctypes.c_double),
+        ("t_end", ctypes.c_double),
     ]
 
 
@@ -124,6 +126,12 @@ _PROTOS = [
     ("mm_solver_stats_get", _I, [_VP, ctypes.POINTER(mm_solver_stats), _VP]),
     ("mm_solver_average_M", _I, [_VP, _DP, _VP]),
     ("mm_solver_relax_norms", _I, [_VP, _DP, _VP]),
+    ("mm_batch_instance_bytes", _I, [ctypes.POINTER(mm_batch_instance), _I, ctypes.POINTER(_SZ),
+                                     ctypes.POINTER(_SZ)]),
+    ("mm_batch_add", _I, [_VP, ctypes.POINTER(mm_batch_instance), _VP, ctypes.POINTER(_I), _VP]),
+    ("mm_batch_remove", _I, [_VP, _I]),
+    ("mm_batch_slot_count", _I, [_VP]),
+    ("mm_batch_stop", _I, [_VP, _I, _VP]),
     ("mm_batch_create", _I, [ctypes.POINTER(_VP), ctypes.POINTER(mm_batch_config), _I,
                              ctypes.POINTER(mm_batch_instance), _VP, _VP]),
     ("mm_batch_destroy", _I, [_VP]),

@@ -1561,7 +1561,7 @@ mm_status conv_execute(ConvPlan *p, const void *M, const uint8_t *regions, const
 
 // ---- grouped convolution: many plans, one launch per pass and transform length -------------------
 // Every member plan uses the power-of-two passes (register z pass included).  The members' blocks
-// of one pass and one length form a work list (member, block); a member whose `active` flag is 0
+// of one pass and one length form a work list (member, block); a member whose run flag is 0
 // skips its blocks, so finished instances drop out without rebuilding the lists.
 namespace {
 
@@ -1574,16 +1574,22 @@ struct GDesc {
 	T *H;
 	const uint8_t *reg;
 	const T *ms_tab;
+	const int *flags;   // the member's run flags: [0] runs, [1] gated runs (NULL: always)
 	int nx, ny, nz, py, hx, lx, qy, qz;
 };
+
+__device__ __forceinline__ bool member_skips(const int *flags, int gate)
+{
+	return flags && (!flags[0] || (gate && !flags[1]));
+}
 
 template <typename T, int N, int LPB>
 __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_grp(const GDesc<T> *__restrict__ d,
                                                                       const int2 *__restrict__ items, int input,
-                                                                      const int *__restrict__ active)
+                                                                      int gate)
 {
 	const int2 it = items[blockIdx.x];
-	if (active && !active[it.x]) return;
+	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
 	x_fwd_ct_body<T, N, LPB, true>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x,
 	                               it.y);
@@ -1591,22 +1597,20 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_grp(const GDe
 
 template <typename T, int N, int LPB>
 __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_grp(const GDesc<T> *__restrict__ d,
-                                                                      const int2 *__restrict__ items,
-                                                                      const int *__restrict__ active)
+                                                                      const int2 *__restrict__ items, int gate)
 {
 	const int2 it = items[blockIdx.x];
-	if (active && !active[it.x]) return;
+	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
 	x_inv_ct_body<T, N, LPB>(g.spec, g.H, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
 }
 
 template <typename T, int N, int TB, bool INV>
 __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_grp(const GDesc<T> *__restrict__ d,
-                                                                    const int2 *__restrict__ items,
-                                                                    const int *__restrict__ active)
+                                                                    const int2 *__restrict__ items, int gate)
 {
 	const int2 it = items[blockIdx.x];
-	if (active && !active[it.x]) return;
+	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
 	const int tiles = (g.hx + TB - 1) / TB;
 	y_ct_body<T, N, TB, INV>(g.spec, INV ? N : g.ny, INV ? g.ny : N, g.hx, g.lx, g.tw_y, it.y % tiles, it.y / tiles);
@@ -1614,10 +1618,10 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_grp(const GDesc
 
 template <typename T, int PZ>
 __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_grp(const GDesc<T> *__restrict__ d, const int2 *__restrict__ items,
-                                                        const int *__restrict__ active)
+                                                        int gate)
 {
 	const int2 it = items[blockIdx.x];
-	if (active && !active[it.x]) return;
+	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
 	const int tiles = (g.hx + 31) / 32;
 	z_reg_body<T, PZ>(g.spec, g.tensor, g.nz, g.py, g.hx, g.lx, g.qy, g.qz, it.y % tiles, it.y / tiles);
@@ -1677,7 +1681,7 @@ mm_status group_smem(int pass, int len)
 }
 
 template <typename T>
-void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, const int *active, cudaStream_t st)
+void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, int gate, cudaStream_t st)
 {
 	using C = cplx<T>;
 	const GDesc<T> *d = (const GDesc<T> *)g->desc;
@@ -1685,19 +1689,19 @@ void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, const
 		constexpr int N = decltype(nc)::value;
 		constexpr int LPB = ct_lpb(N, sizeof(C)), TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
 		const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
-		if (l.pass == 0) k_x_fwd_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, input, active);
-		if (l.pass == 4) k_x_inv_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, active);
-		if (l.pass == 1) k_y_grp<T, N, TB, false><<<l.n, TB * TPL, sy, st>>>(d, l.items, active);
-		if (l.pass == 3) k_y_grp<T, N, TB, true><<<l.n, TB * TPL, sy, st>>>(d, l.items, active);
+		if (l.pass == 0) k_x_fwd_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, input, gate);
+		if (l.pass == 4) k_x_inv_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, gate);
+		if (l.pass == 1) k_y_grp<T, N, TB, false><<<l.n, TB * TPL, sy, st>>>(d, l.items, gate);
+		if (l.pass == 3) k_y_grp<T, N, TB, true><<<l.n, TB * TPL, sy, st>>>(d, l.items, gate);
 	};
 	if (l.pass == 2) {
 		const size_t sz = (size_t)2 * l.len * 96 * sizeof(C);
 		switch (l.len) {
-		case 2: k_z_grp<T, 2><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
-		case 4: k_z_grp<T, 4><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
-		case 8: k_z_grp<T, 8><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
-		case 16: k_z_grp<T, 16><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); break;
-		case 32: if constexpr (sizeof(T) == 4) { k_z_grp<T, 32><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, active); } break;
+		case 2: k_z_grp<T, 2><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
+		case 4: k_z_grp<T, 4><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
+		case 8: k_z_grp<T, 8><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
+		case 16: k_z_grp<T, 16><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
+		case 32: if constexpr (sizeof(T) == 4) { k_z_grp<T, 32><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); } break;
 		}
 		return;
 	}
@@ -1734,6 +1738,7 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		d.H = (T *)m[i].H;
 		d.reg = m[i].reg;
 		d.ms_tab = (const T *)m[i].ms_tab;
+		d.flags = m[i].flags;
 		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
 		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
 		using C = cplx<T>;
@@ -1786,12 +1791,12 @@ mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int
 	return MM_OK;
 }
 
-mm_status conv_group_execute(ConvGroup *g, int input, const int *active_device, cudaStream_t st)
+mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st)
 {
 	if (!g || input < 0 || input > 2) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad input selector");
 	for (const auto &l : g->lists) {
-		if (g->prec == MM_F64) group_launch<double>(g, l, input, active_device, st);
-		else group_launch<float>(g, l, input, active_device, st);
+		if (g->prec == MM_F64) group_launch<double>(g, l, input, gate, st);
+		else group_launch<float>(g, l, input, gate, st);
 		MM_TRY(after_launch("k_conv_grp"));
 	}
 	return MM_OK;

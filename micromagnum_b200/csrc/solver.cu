@@ -1426,15 +1426,27 @@ MM_API mm_status mm_solver_average_M(mm_solver *s, double *avg3, void *stream)
 } // extern "C"
 
 // ================================================================================================
-// Batched relaxations: many independent instances of uneven size advance in lock step, one
-// Runge-Kutta attempt per round for every active instance.  Each instance is a full solver
-// (own state, stages, tensor and spectra); the rounds run as grouped launches (one per pass and
-// transform length for the convolution, one per stage for the fused stage kernel) over work
-// lists of (instance, tile), and the step controller, the accept step and the relaxation check
-// run on the device per instance, so a captured round needs no host decision.
+// Batched solves: many independent instances of uneven size advance in lock step, one
+// Runge-Kutta attempt per round for every running instance.  Each instance is a full solver (own
+// state, stages, tensor and spectra); a round runs as grouped launches (one per pass and transform
+// length for the convolution, one per stage for the fused stage kernel) over work lists of
+// (instance, tile), and the step controller, the accept step and the stop test run on the device
+// per instance, so a captured round needs no host decision.  Instances join and leave between
+// rounds (slots); the work lists and the captured rounds are rebuilt when the membership changes.
 // ================================================================================================
 namespace mm {
 namespace {
+
+// Device bookkeeping of one instance.
+struct BState {
+	int steps, attempts, rejected, status;  // status: 0 running, 1 finished, 2 non-finite state
+	double t, h;
+};
+struct BSlot {
+	BState bs;
+	int active;  // takes part in rounds
+	int need_k0; // the next round evaluates k_0 at the state (after set-up or a new state)
+};
 
 template <typename T>
 struct BDesc {
@@ -1442,6 +1454,8 @@ struct BDesc {
 	T *m, *m_lo, *ys[2], *hd, *ynew_lo;
 	KTab<T> *kt;
 	DevState *ds;
+	BSlot *slot;
+	double t_end;  // > 0: stop at this time (clamping the last step); 0: stop on the torque test
 	int n, tiles_x, tiles_y, ntiles;
 };
 
@@ -1449,14 +1463,14 @@ constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage
 constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
 
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
+// K0: the k_0 evaluation of instances that need it (others skip it).
 template <typename T, bool COMP, int S, bool TORQUE>
 __global__ void __launch_bounds__(256, stage_min_blocks<T>())
-    k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items,
-                const int *__restrict__ active)
+    k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items)
 {
 	const int2 it = items[blockIdx.x];
-	if (!active[it.x]) return;
 	const BDesc<T> &g = d[it.x];
+	if (!g.slot->active || (S == 0 && !g.slot->need_k0)) return;
 	__shared__ CellArgs<T> a;
 	__shared__ T msr[256];
 	if (threadIdx.x == 0 && threadIdx.y == 0) a = g.a;
@@ -1475,14 +1489,15 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 	if (TORQUE) block_max_to(&g.ds->max_tq2, tq2);
 }
 
-// Grouped first-same-as-last first stage, y_1 = y_n + h b_10 k_0, into ys[0].
+// Grouped first-same-as-last first stage, y_1 = y_n + h b_10 k_0, into ys[0] (instances whose
+// k_0 is the previous attempt's last stage).
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(256) k_prepare1_grp(const BDesc<T> *__restrict__ d, double b10,
-                                                      const int2 *__restrict__ items, const int *__restrict__ active)
+                                                      const int2 *__restrict__ items)
 {
 	const int2 it = items[blockIdx.x];
-	if (!active[it.x]) return;
 	const BDesc<T> &g = d[it.x];
+	if (!g.slot->active || g.slot->need_k0) return;
 	const size_t n3 = 3 * (size_t)g.n;
 	const T f = (T)(g.ds->h * b10);
 	const T *k0 = g.kt->k[0];
@@ -1508,25 +1523,21 @@ __global__ void __launch_bounds__(256) k_accept_grp(const BDesc<T> *__restrict__
 		accept_cell<T, COMP>(n, ynew, g.ynew_lo, g.m, g.m_lo, i);
 }
 
-// Per-instance bookkeeping of a batch (device; copied to the host on request).
-struct BState {
-	int steps, attempts, rejected, status;  // status: 0 running, 1 relaxed, 2 non-finite state
-	double t, h;
-};
-
 // Grouped step controller (one thread per instance): the single-instance controller's decision,
-// then time and step-size update, counters, and the relaxation check on the accepted state
-// (its torque was reduced by the last stage, whose input is y_{n+1} for a first-same-as-last
-// tableau).  Finished instances leave `active`; the accept kernel still applies their last step.
+// then time and step-size update, counters, and the stop test on the accepted state: t >= t_end
+// for a timed solve (the step before t_end is clamped onto it), else max |m x H_eff| / Ms below
+// the threshold at a multiple of check_every accepted steps (its torque was reduced by the last
+// stage, whose input is y_{n+1} for a first-same-as-last tableau).  A finished instance leaves
+// the rounds; the accept kernel still applies its last step.
 template <typename T>
 __global__ void k_controller_grp(const BDesc<T> *__restrict__ d, int count, double eps_abs, double eps_rel,
-                                 int order, int fsal, int s, double tq_thr2, int check_every, BState *bs,
-                                 int *active)
+                                 int order, int fsal, int s, double tq_thr2, int check_every)
 {
 	const int i = blockIdx.x * blockDim.x + threadIdx.x;
 	if (i >= count) return;
 	DevState *st = d[i].ds;
-	if (!active[i]) {
+	BSlot *sl = d[i].slot;
+	if (!sl->active) {
 		st->accept = 0;
 		return;
 	}
@@ -1534,89 +1545,116 @@ __global__ void k_controller_grp(const BDesc<T> *__restrict__ d, int count, doub
 	const double tq2 = st->max_tq2;
 	st->max_tq2 = 0.0;
 	control_attempt<T>(st, d[i].kt, eps_abs, eps_rel, order, fsal, s, nullptr, nullptr);
-	BState &b = bs[i];
+	BState &b = sl->bs;
 	b.attempts++;
+	sl->need_k0 = 0;
+	const double t_end = d[i].t_end;
 	if (st->not_finite) {
 		b.status = 2;
-		active[i] = 0;
+		sl->active = 0;
 		st->accept = 0;
 	} else if (st->accept) {
 		st->t += h;
 		st->h = st->h_new;
 		b.steps++;
-		if (check_every > 0 && b.steps % check_every == 0 && tq2 < tq_thr2) {
+		if (t_end > 0.0) {
+			if (st->t >= t_end) {
+				b.status = 1;
+				sl->active = 0;
+			} else if (st->t + st->h > t_end) {
+				st->h = t_end - st->t;
+			}
+		} else if (check_every > 0 && b.steps % check_every == 0 && tq2 < tq_thr2) {
 			b.status = 1;
-			active[i] = 0;
+			sl->active = 0;
 		}
 	} else {
 		st->h = st->h_new;
 		b.rejected++;
+		if (t_end > 0.0 && st->t + st->h > t_end) st->h = t_end - st->t;
 	}
 	b.t = st->t;
 	b.h = st->h;
 }
 
-// Resets time, step size, counters and reductions of every instance (start of a relaxation).
-__global__ void k_batch_reset(DevState *const *ds, int count, double h0, BState *bs, int *active)
+// (Re)starts one instance: t = 0, step size h0 (clamped to t_end), counters and reductions
+// cleared, k_0 to be evaluated by the next round.
+__global__ void k_slot_start(DevState *st, BSlot *sl, double h0, double t_end)
 {
-	const int i = blockIdx.x * blockDim.x + threadIdx.x;
-	if (i >= count) return;
-	DevState *st = ds[i];
+	const double h = (t_end > 0.0 && h0 > t_end) ? t_end : h0;
 	st->t = 0.0;
-	st->h = h0;
+	st->h = h;
 	st->max_err2 = st->max_k02 = st->max_tq2 = 0.0;
 	st->accept = 0;
 	st->not_finite = 0;
-	bs[i] = BState{0, 0, 0, 0, 0.0, h0};
-	active[i] = 1;
+	sl->bs = BState{0, 0, 0, 0, 0.0, h};
+	sl->active = 1;
+	sl->need_k0 = 1;
 }
+
+// Stops an instance (its slot keeps its results).
+__global__ void k_slot_stop(BSlot *sl) { sl->active = 0; }
 
 } // namespace
 } // namespace mm
 
 struct mm_batch {
-	int count = 0;
 	int prec = MM_F32;
 	mm_batch_config cfg{};
-	std::vector<mm_solver *> inst;
+	struct Slot {
+		mm_solver *s = nullptr;  // nullptr: free slot
+		mm::BSlot *dev = nullptr;
+		double t_end = 0.0;
+	};
+	std::vector<Slot> slots;
+	std::vector<int> members;                     // slot index of each member of the built rounds
+	bool dirty = true;                            // membership changed since the rounds were built
+	bool any_need_k0 = false;                     // some member starts with the next round
 	mm::ConvGroup *conv = nullptr;
-	void *desc = nullptr;                         // BDesc<T>[count]
-	mm::DevState **ds_list = nullptr;             // device array of the instances' DevState pointers
+	void *desc = nullptr;                         // BDesc<T>[members]
 	int2 *stage_items = nullptr, *cell3_items = nullptr, *cell_items = nullptr;
 	int n_stage = 0, n_cell3 = 0, n_cell = 0;
-	int *active = nullptr;
-	mm::BState *bs = nullptr;
-	mm::BState *bs_h = nullptr;                   // pinned
-	int *active_h = nullptr;                      // pinned
-	bool need_first = true;                       // next round evaluates k_0 (after a reset)
+	mm::BSlot *slots_h = nullptr;                 // pinned copies for result queries
+	size_t slots_h_cap = 0;
 	cudaStream_t gs = nullptr;
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // [0] first round (k_0 evaluated), [1] later rounds
+	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // [0] with k_0 evaluation, [1] without
 	int launches_per_round[2] = {0, 0};
 };
 
 namespace mm {
 namespace {
 
-void free_batch(mm_batch *b)
+void drop_rounds(mm_batch *b)
 {
-	if (!b) return;
 	for (auto &g : b->gexec)
 		if (g) cudaGraphExecDestroy(g);
-	if (b->gs) cudaStreamDestroy(b->gs);
-	if (b->ev_in) cudaEventDestroy(b->ev_in);
-	if (b->ev_out) cudaEventDestroy(b->ev_out);
+	b->gexec[0] = b->gexec[1] = nullptr;
 	conv_group_destroy(b->conv);
+	b->conv = nullptr;
 	cudaFree(b->desc);
-	cudaFree(b->ds_list);
 	cudaFree(b->stage_items);
 	cudaFree(b->cell3_items);
 	cudaFree(b->cell_items);
-	cudaFree(b->active);
-	cudaFree(b->bs);
-	cudaFreeHost(b->bs_h);
-	cudaFreeHost(b->active_h);
-	for (mm_solver *s : b->inst) free_solver(s);
+	b->desc = nullptr;
+	b->stage_items = b->cell3_items = b->cell_items = nullptr;
+	b->n_stage = b->n_cell3 = b->n_cell = 0;
+	b->members.clear();
+}
+
+void free_batch(mm_batch *b)
+{
+	if (!b) return;
+	if (b->gs) cudaStreamSynchronize(b->gs);
+	drop_rounds(b);
+	if (b->gs) cudaStreamDestroy(b->gs);
+	if (b->ev_in) cudaEventDestroy(b->ev_in);
+	if (b->ev_out) cudaEventDestroy(b->ev_out);
+	cudaFreeHost(b->slots_h);
+	for (auto &sl : b->slots) {
+		free_solver(sl.s);
+		cudaFree(sl.dev);
+	}
 	delete b;
 }
 
@@ -1625,9 +1663,9 @@ void launch_stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, c
 {
 	const BDesc<T> *d = (const BDesc<T> *)b->desc;
 	if (sc.last)
-		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items, b->active);
+		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items);
 	else
-		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items, b->active);
+		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items);
 }
 
 template <typename T, bool COMP>
@@ -1646,27 +1684,27 @@ mm_status stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, cud
 	return after_launch("k_stage_grp");
 }
 
-// One lock-step round: an attempt of every active instance, its controller decision and the
-// accept step.  first: k_0 is evaluated at the state (start of a relaxation); otherwise it is the
-// previous attempt's last stage (first same as last, also after a rejection, like the reference).
+// One lock-step round over the members: an attempt each, the controller decision and the accept
+// step.  with_k0: instances flagged need_k0 evaluate k_0 at their state first; the others take
+// it from the previous attempt's last stage (first same as last, also after a rejection, like
+// the reference).
 template <typename T>
-mm_status batch_round(mm_batch *b, bool first, cudaStream_t st)
+mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 {
 	constexpr bool COMP = sizeof(T) == 4;
-	const Tableau &tb = b->inst[0]->tab;
-	if (first) {
+	const Tableau tb = make_tableau(MM_RK_DP54);
+	const BDesc<T> *d = (const BDesc<T> *)b->desc;
+	if (with_k0) {
 		StageCoef sc{};
 		sc.stage = 0;
 		sc.a_i = tb.a[0];
 		sc.write_next = 1;
 		sc.bn[0] = tb.b[1][0];
-		MM_TRY(conv_group_execute(b->conv, 0, b->active, st));
+		MM_TRY(conv_group_execute(b->conv, 0, 1, st));
 		MM_TRY((stage_grp<T, COMP>(b, sc, 0, 0, st)));
-	} else {
-		k_prepare1_grp<T, COMP><<<b->n_cell3, 256, 0, st>>>((const BDesc<T> *)b->desc, tb.b[1][0], b->cell3_items,
-		                                                   b->active);
-		MM_TRY(after_launch("k_prepare1_grp"));
 	}
+	k_prepare1_grp<T, COMP><<<b->n_cell3, 256, 0, st>>>(d, tb.b[1][0], b->cell3_items);
+	MM_TRY(after_launch("k_prepare1_grp"));
 	int last_buf = 0;
 	for (int i = 1; i < tb.s; ++i) {
 		StageCoef sc{};
@@ -1685,21 +1723,21 @@ mm_status batch_round(mm_batch *b, bool first, cudaStream_t st)
 			}
 		}
 		const int in = 1 + ((i - 1) & 1);
-		MM_TRY(conv_group_execute(b->conv, in, b->active, st));
+		MM_TRY(conv_group_execute(b->conv, in, 0, st));
 		MM_TRY((stage_grp<T, COMP>(b, sc, in, i & 1, st)));
 		if (sc.last) last_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
 	}
 	const double thr = b->cfg.max_torque;
-	k_controller_grp<T><<<(b->count + 127) / 128, 128, 0, st>>>(
-	    (const BDesc<T> *)b->desc, b->count, b->cfg.eps_abs, b->cfg.eps_rel, tb.order, tb.fsal, tb.s, thr * thr,
-	    b->cfg.check_every_nth_step, b->bs, b->active);
+	const int count = (int)b->members.size();
+	k_controller_grp<T><<<(count + 127) / 128, 128, 0, st>>>(d, count, b->cfg.eps_abs, b->cfg.eps_rel, tb.order, tb.fsal,
+	                                                        tb.s, thr * thr, b->cfg.check_every_nth_step);
 	MM_TRY(after_launch("k_controller_grp"));
-	k_accept_grp<T, COMP><<<b->n_cell, 256, 0, st>>>((const BDesc<T> *)b->desc, last_buf, b->cell_items);
+	k_accept_grp<T, COMP><<<b->n_cell, 256, 0, st>>>(d, last_buf, b->cell_items);
 	MM_TRY(after_launch("k_accept_grp"));
 	return MM_OK;
 }
 
-// Captures one round (first or later) into a graph on the batch's private stream.
+// Captures one round into a graph on the batch's private stream.
 template <typename T>
 mm_status batch_graph(mm_batch *b, int v)
 {
@@ -1721,16 +1759,21 @@ mm_status batch_graph(mm_batch *b, int v)
 	return MM_OK;
 }
 
+// Work lists, descriptors, grouped convolution and captured rounds of the current members.
 template <typename T>
-mm_status batch_setup(mm_batch *b, cudaStream_t st)
+mm_status build_rounds(mm_batch *b, cudaStream_t st)
 {
-	std::vector<BDesc<T>> h(b->count);
-	std::vector<ConvGroupMember> mem(b->count);
-	std::vector<DevState *> dsl(b->count);
+	drop_rounds(b);
+	std::vector<BDesc<T>> h;
+	std::vector<ConvGroupMember> mem;
 	std::vector<int2> si, c3, c1;
-	for (int i = 0; i < b->count; ++i) {
-		mm_solver *s = b->inst[i];
-		BDesc<T> &d = h[i];
+	for (int k = 0; k < (int)b->slots.size(); ++k) {
+		const mm_batch::Slot &sl = b->slots[k];
+		if (!sl.s) continue;
+		mm_solver *s = sl.s;
+		const int i = (int)b->members.size();
+		b->members.push_back(k);
+		BDesc<T> d{};
 		d.a = args_of<T>(s);
 		d.m = (T *)s->m;
 		d.m_lo = (T *)s->m_lo;
@@ -1740,44 +1783,120 @@ mm_status batch_setup(mm_batch *b, cudaStream_t st)
 		d.ynew_lo = (T *)s->ynew_lo;
 		d.kt = (KTab<T> *)s->ktab;
 		d.ds = s->dst;
+		d.slot = sl.dev;
+		d.t_end = sl.t_end;
 		d.n = (int)s->n;
 		const dim3 tg = stage_grid(s->cfg);
 		d.tiles_x = (int)tg.x;
 		d.tiles_y = (int)tg.y;
 		d.ntiles = (int)(tg.x * tg.y * tg.z);
+		h.push_back(d);
 		for (int t = 0; t < d.ntiles; t += BATCH_TILES) si.push_back(make_int2(i, t));
-		for (int c = 0; c * (size_t)BATCH_CHUNK < 3 * s->n; ++c) c3.push_back(make_int2(i, c));
-		for (int c = 0; c * (size_t)BATCH_CHUNK < s->n; ++c) c1.push_back(make_int2(i, c));
-		mem[i] = ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1]}, s->hd, s->reg, s->ms_tab};
-		dsl[i] = s->dst;
+		for (int c = 0; (size_t)c * BATCH_CHUNK < 3 * s->n; ++c) c3.push_back(make_int2(i, c));
+		for (int c = 0; (size_t)c * BATCH_CHUNK < s->n; ++c) c1.push_back(make_int2(i, c));
+		mem.push_back(ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1]}, s->hd, s->reg, s->ms_tab, &sl.dev->active});
 	}
-	MM_TRY(conv_group_create(&b->conv, mem.data(), b->count, st));
+	b->dirty = false;
+	if (b->members.empty()) return MM_OK;
+	MM_TRY(conv_group_create(&b->conv, mem.data(), (int)mem.size(), st));
 	auto up = [&](void **dst, const void *src, size_t bytes) -> mm_status {
 		MM_CUDA(cudaMalloc(dst, bytes));
 		MM_CUDA(cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, st));
 		return MM_OK;
 	};
-	MM_TRY(up(&b->desc, h.data(), sizeof(BDesc<T>) * b->count));
-	MM_TRY(up((void **)&b->ds_list, dsl.data(), sizeof(DevState *) * b->count));
+	MM_TRY(up(&b->desc, h.data(), sizeof(BDesc<T>) * h.size()));
 	MM_TRY(up((void **)&b->stage_items, si.data(), sizeof(int2) * si.size()));
 	MM_TRY(up((void **)&b->cell3_items, c3.data(), sizeof(int2) * c3.size()));
 	MM_TRY(up((void **)&b->cell_items, c1.data(), sizeof(int2) * c1.size()));
 	b->n_stage = (int)si.size();
 	b->n_cell3 = (int)c3.size();
 	b->n_cell = (int)c1.size();
-	MM_CUDA(cudaMalloc(&b->active, sizeof(int) * b->count));
-	MM_CUDA(cudaMalloc(&b->bs, sizeof(BState) * b->count));
-	MM_CUDA(cudaMallocHost(&b->bs_h, sizeof(BState) * b->count));
-	MM_CUDA(cudaMallocHost(&b->active_h, sizeof(int) * b->count));
-	MM_CUDA(cudaStreamCreateWithFlags(&b->gs, cudaStreamNonBlocking));
-	MM_CUDA(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming));
-	MM_CUDA(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming));
-	k_batch_reset<<<(b->count + 127) / 128, 128, 0, st>>>(b->ds_list, b->count, b->cfg.h0, b->bs, b->active);
-	MM_TRY(after_launch("k_batch_reset"));
 	MM_CUDA(cudaStreamSynchronize(st));
 	MM_TRY(batch_graph<T>(b, 0));
 	MM_TRY(batch_graph<T>(b, 1));
 	return MM_OK;
+}
+
+// Device bytes of one instance: resident (state, stage vectors, spectra, tensor spectrum) and the
+// extra transient peak of its set-up (the FP64 tensor and its FFT workspace).
+void instance_bytes(const mm_batch_instance &q, int prec, size_t *resident, size_t *transient)
+{
+	const size_t s = prec == MM_F32 ? 4 : 8, n = (size_t)q.nx * q.ny * q.nz;
+	const int px = mm_round_tensor_dimension(q.nx, 0, MM_PADDING_ROUND_POT);
+	const int py = mm_round_tensor_dimension(q.ny, 0, MM_PADDING_ROUND_POT);
+	int pz = mm_round_tensor_dimension(q.nz, 0, MM_PADDING_ROUND_POT);
+	if (pz < 2) pz = 2;
+	const size_t hx = px / 2 + 1, qy = py / 2 + 1, qz = pz / 2 + 1;
+	const size_t E = prec == MM_F32 ? 1 : 2;
+	size_t w = hx * E;
+	const size_t nb = (w + 255) / 256;
+	w = (w + 2 * nb - 1) / (2 * nb) * (2 * nb);
+	const size_t lx = w / E;
+	const size_t vecs = (prec == MM_F32 ? 3 : 1) + 2 + 7 + 1;  // m (+lo, ynew_lo), ys[2], k[7], H_demag
+	*resident = vecs * 3 * n * s + n + 3 * (size_t)q.nz * py * lx * 2 * s + 6 * qz * qy * hx * s + (1 << 16);
+	*transient = 6 * (size_t)px * py * pz * 8 + (size_t)px * py * pz * 16;
+}
+
+template <typename T>
+mm_status add_instance(mm_batch *b, const mm_batch_instance &q, const uint8_t *mask, int *slot_out,
+                       cudaStream_t st)
+{
+	mm_solver_config c{};
+	c.nx = q.nx; c.ny = q.ny; c.nz = q.nz;
+	c.dx = q.dx; c.dy = q.dy; c.dz = q.dz;
+	c.precision = b->prec;
+	c.tableau = MM_RK_DP54;
+	c.terms = MM_TERM_DEMAG | MM_TERM_EXCHANGE;
+	bool zeeman = false;
+	for (int k = 0; k < 3; ++k) {
+		c.H_ext[k] = q.H_ext[k];
+		c.H_pulse[k] = q.H_pulse[k];
+		zeeman = zeeman || q.H_ext[k] != 0.0 || q.H_pulse[k] != 0.0;
+	}
+	if (zeeman) c.terms |= MM_TERM_ZEEMAN;
+	c.pulse_rise = q.pulse_rise;
+	c.do_precess = 1;
+	c.zl_do_precess = 1;
+	c.padding = MM_PADDING_ROUND_POT;
+	c.eps_abs = b->cfg.eps_abs;
+	c.eps_rel = b->cfg.eps_rel;
+	c.h0 = b->cfg.h0;
+	c.fsal_reuse_after_reject = 1;
+	mm_material mats[2] = {};
+	mats[1].Ms = q.Ms;
+	mats[1].A = q.A;
+	mats[1].alpha = q.alpha;
+	mats[0].alpha = q.alpha;
+	const size_t n = (size_t)q.nx * q.ny * q.nz;
+	std::vector<uint8_t> ones;
+	if (!mask) {
+		ones.assign(n, 1);
+		mask = ones.data();
+	}
+	mm_solver *s = nullptr;
+	MM_TRY(solver_create(&s, &c, 2, mats, mask, nullptr, st, 2));
+	BSlot *dev = nullptr;
+	const cudaError_t e = cudaMalloc(&dev, sizeof(BSlot));
+	if (e != cudaSuccess) {
+		free_solver(s);
+		return cuda_status(e, "cudaMalloc");
+	}
+	cudaMemsetAsync(dev, 0, sizeof(BSlot), st);  // not running until it gets a state
+	int k = 0;
+	while (k < (int)b->slots.size() && b->slots[k].s) ++k;
+	if (k == (int)b->slots.size()) b->slots.emplace_back();
+	b->slots[k].s = s;
+	b->slots[k].dev = dev;
+	b->slots[k].t_end = q.t_end;
+	b->dirty = true;
+	*slot_out = k;
+	MM_CUDA(cudaStreamSynchronize(st));
+	return MM_OK;
+}
+
+mm_batch::Slot *slot_of(mm_batch *b, int k)
+{
+	return (b && k >= 0 && k < (int)b->slots.size() && b->slots[k].s) ? &b->slots[k] : nullptr;
 }
 
 } // namespace
@@ -1785,10 +1904,20 @@ mm_status batch_setup(mm_batch *b, cudaStream_t st)
 
 extern "C" {
 
+MM_API mm_status mm_batch_instance_bytes(const mm_batch_instance *instance, int precision, size_t *resident,
+                                         size_t *transient)
+{
+	if (!instance || !resident || !transient || (precision != MM_F64 && precision != MM_F32))
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_instance_bytes: invalid argument");
+	instance_bytes(*instance, precision, resident, transient);
+	return MM_OK;
+}
+
 MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *cfg, int count,
                                  const mm_batch_instance *inst_host, const uint8_t *masks_host, void *stream)
 {
-	if (!out || !cfg || count < 1 || !inst_host) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid argument");
+	if (!out || !cfg || count < 0 || (count > 0 && !inst_host))
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid argument");
 	if (cfg->precision != MM_F64 && cfg->precision != MM_F32)
 		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid precision");
 	if (!(cfg->eps_abs > 0) || !(cfg->eps_rel > 0) || !(cfg->h0 > 0) || !(cfg->max_torque >= 0) ||
@@ -1796,47 +1925,18 @@ MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *cfg, int
 		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_create: invalid tolerances, h0, torque or check interval");
 	cudaStream_t st = as_stream(stream);
 	mm_batch *b = new mm_batch();
-	b->count = count;
 	b->prec = cfg->precision;
 	b->cfg = *cfg;
+	mm_status r = cuda_status(cudaStreamCreateWithFlags(&b->gs, cudaStreamNonBlocking), "cudaStreamCreate");
+	if (r == MM_OK) r = cuda_status(cudaEventCreateWithFlags(&b->ev_in, cudaEventDisableTiming), "cudaEventCreate");
+	if (r == MM_OK) r = cuda_status(cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming), "cudaEventCreate");
 	size_t off = 0;
-	for (int i = 0; i < count && true; ++i) {
-		const mm_batch_instance &q = inst_host[i];
-		mm_solver_config c{};
-		c.nx = q.nx; c.ny = q.ny; c.nz = q.nz;
-		c.dx = q.dx; c.dy = q.dy; c.dz = q.dz;
-		c.precision = cfg->precision;
-		c.tableau = MM_RK_DP54;
-		c.terms = MM_TERM_DEMAG | MM_TERM_EXCHANGE;
-		c.do_precess = 1;
-		c.zl_do_precess = 1;
-		c.padding = MM_PADDING_ROUND_POT;
-		c.eps_abs = cfg->eps_abs;
-		c.eps_rel = cfg->eps_rel;
-		c.h0 = cfg->h0;
-		c.fsal_reuse_after_reject = 1;
-		mm_material mats[2] = {};
-		mats[1].Ms = q.Ms;
-		mats[1].A = q.A;
-		mats[1].alpha = q.alpha;
-		mats[0].alpha = q.alpha;
-		const size_t n = (size_t)q.nx * q.ny * q.nz;
-		std::vector<uint8_t> ones;
-		const uint8_t *reg = masks_host ? masks_host + off : nullptr;
-		if (!reg) {
-			ones.assign(n, 1);
-			reg = ones.data();
-		}
-		off += n;
-		mm_solver *s = nullptr;
-		const mm_status r = solver_create(&s, &c, 2, mats, reg, nullptr, stream, 2);
-		if (r != MM_OK) {
-			free_batch(b);
-			return r;
-		}
-		b->inst.push_back(s);
+	for (int i = 0; i < count && r == MM_OK; ++i) {
+		int slot = 0;
+		r = b->prec == MM_F64 ? add_instance<double>(b, inst_host[i], masks_host ? masks_host + off : nullptr, &slot, st)
+		                      : add_instance<float>(b, inst_host[i], masks_host ? masks_host + off : nullptr, &slot, st);
+		off += (size_t)inst_host[i].nx * inst_host[i].ny * inst_host[i].nz;
 	}
-	const mm_status r = b->prec == MM_F64 ? batch_setup<double>(b, st) : batch_setup<float>(b, st);
 	if (r != MM_OK) {
 		free_batch(b);
 		return r;
@@ -1851,20 +1951,58 @@ MM_API mm_status mm_batch_destroy(mm_batch *b)
 	return MM_OK;
 }
 
-MM_API mm_status mm_batch_set_M(mm_batch *b, int index, const double *M_device, void *stream)
+MM_API mm_status mm_batch_add(mm_batch *b, const mm_batch_instance *instance, const uint8_t *mask_host,
+                              int *slot_out, void *stream)
 {
-	if (!b || index < 0 || index >= b->count || !M_device)
-		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_set_M: invalid argument");
-	MM_TRY(mm_solver_set_M(b->inst[index], M_device, stream));
-	b->need_first = true;
+	if (!b || !instance || !slot_out) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_add: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	return b->prec == MM_F64 ? add_instance<double>(b, *instance, mask_host, slot_out, st)
+	                         : add_instance<float>(b, *instance, mask_host, slot_out, st);
+}
+
+MM_API mm_status mm_batch_remove(mm_batch *b, int slot)
+{
+	mm_batch::Slot *sl = slot_of(b, slot);
+	if (!sl) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_remove: no such slot");
+	MM_CUDA(cudaStreamSynchronize(b->gs));
+	free_solver(sl->s);
+	cudaFree(sl->dev);
+	*sl = mm_batch::Slot{};
+	b->dirty = true;
 	return MM_OK;
 }
 
-MM_API mm_status mm_batch_get_M(mm_batch *b, int index, double *M_device, void *stream)
+MM_API int mm_batch_slot_count(mm_batch *b) { return b ? (int)b->slots.size() : 0; }
+
+MM_API mm_status mm_batch_set_M(mm_batch *b, int slot, const double *M_device, void *stream)
 {
-	if (!b || index < 0 || index >= b->count || !M_device)
-		return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_get_M: invalid argument");
-	return mm_solver_get_M(b->inst[index], M_device, stream);
+	mm_batch::Slot *sl = slot_of(b, slot);
+	if (!sl || !M_device) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_set_M: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	MM_CUDA(cudaStreamSynchronize(b->gs));
+	MM_TRY(mm_solver_set_M(sl->s, M_device, stream));
+	k_slot_start<<<1, 1, 0, st>>>(sl->s->dst, sl->dev, b->cfg.h0, sl->t_end);
+	MM_TRY(after_launch("k_slot_start"));
+	MM_CUDA(cudaStreamSynchronize(st));
+	b->any_need_k0 = true;
+	return MM_OK;
+}
+
+MM_API mm_status mm_batch_get_M(mm_batch *b, int slot, double *M_device, void *stream)
+{
+	mm_batch::Slot *sl = slot_of(b, slot);
+	if (!sl || !M_device) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_get_M: invalid argument");
+	MM_CUDA(cudaStreamSynchronize(b->gs));
+	return mm_solver_get_M(sl->s, M_device, stream);
+}
+
+MM_API mm_status mm_batch_stop(mm_batch *b, int slot, void *stream)
+{
+	mm_batch::Slot *sl = slot_of(b, slot);
+	if (!sl) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_stop: no such slot");
+	MM_CUDA(cudaStreamSynchronize(b->gs));
+	k_slot_stop<<<1, 1, 0, as_stream(stream)>>>(sl->dev);
+	return after_launch("k_slot_stop");
 }
 
 MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_interval, long long *rounds_out,
@@ -1872,43 +2010,58 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 {
 	if (!b || max_rounds < 0 || check_interval < 1) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_relax: invalid argument");
 	cudaStream_t st = as_stream(stream);
-	if (b->need_first) {
-		k_batch_reset<<<(b->count + 127) / 128, 128, 0, st>>>(b->ds_list, b->count, b->cfg.h0, b->bs, b->active);
-		MM_TRY(after_launch("k_batch_reset"));
-	}
-	MM_CUDA(cudaEventRecord(b->ev_in, st));
-	MM_CUDA(cudaStreamWaitEvent(b->gs, b->ev_in, 0));
+	if (b->dirty) MM_TRY(b->prec == MM_F64 ? build_rounds<double>(b, st) : build_rounds<float>(b, st));
 	long long done = 0;
-	while (done < max_rounds) {
-		const int v = b->need_first ? 0 : 1;
-		MM_CUDA(cudaGraphLaunch(b->gexec[v], b->gs));
-		launch_counter().fetch_add(b->launches_per_round[v]);
-		b->need_first = false;
-		++done;
-		if (done % check_interval == 0 || done == max_rounds) {
-			MM_CUDA(cudaMemcpyAsync(b->active_h, b->active, sizeof(int) * b->count, cudaMemcpyDeviceToHost, b->gs));
-			MM_CUDA(cudaStreamSynchronize(b->gs));
-			int left = 0;
-			for (int i = 0; i < b->count; ++i) left += b->active_h[i];
-			if (!left) break;
+	if (!b->members.empty()) {
+		const size_t cnt = b->members.size();
+		if (b->slots_h_cap < cnt) {
+			cudaFreeHost(b->slots_h);
+			b->slots_h = nullptr;
+			MM_CUDA(cudaMallocHost(&b->slots_h, sizeof(BSlot) * cnt));
+			b->slots_h_cap = cnt;
 		}
+		MM_CUDA(cudaEventRecord(b->ev_in, st));
+		MM_CUDA(cudaStreamWaitEvent(b->gs, b->ev_in, 0));
+		while (done < max_rounds) {
+			const int v = b->any_need_k0 ? 0 : 1;
+			MM_CUDA(cudaGraphLaunch(b->gexec[v], b->gs));
+			launch_counter().fetch_add(b->launches_per_round[v]);
+			b->any_need_k0 = false;
+			++done;
+			if (done % check_interval == 0 || done == max_rounds) {
+				for (size_t i = 0; i < cnt; ++i)
+					MM_CUDA(cudaMemcpyAsync(&b->slots_h[i], b->slots[b->members[i]].dev, sizeof(BSlot),
+					                        cudaMemcpyDeviceToHost, b->gs));
+				MM_CUDA(cudaStreamSynchronize(b->gs));
+				int left = 0;
+				for (size_t i = 0; i < cnt; ++i) left += b->slots_h[i].active;
+				if (!left) break;
+			}
+		}
+		MM_CUDA(cudaEventRecord(b->ev_out, b->gs));
+		MM_CUDA(cudaStreamWaitEvent(st, b->ev_out, 0));
 	}
-	MM_CUDA(cudaEventRecord(b->ev_out, b->gs));
-	MM_CUDA(cudaStreamWaitEvent(st, b->ev_out, 0));
 	MM_CUDA(cudaStreamSynchronize(st));
 	if (rounds_out) *rounds_out = done;
 	return MM_OK;
 }
 
+// Results of every slot (status -1 for a free slot).
 MM_API mm_status mm_batch_results(mm_batch *b, mm_batch_result *out_host, void *stream)
 {
 	if (!b || !out_host) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_results: invalid argument");
 	cudaStream_t st = as_stream(stream);
-	MM_CUDA(cudaMemcpyAsync(b->bs_h, b->bs, sizeof(BState) * b->count, cudaMemcpyDeviceToHost, st));
-	MM_CUDA(cudaStreamSynchronize(st));
-	for (int i = 0; i < b->count; ++i) {
-		const BState &s = b->bs_h[i];
-		out_host[i] = mm_batch_result{s.status, s.steps, s.attempts, s.rejected, s.t, s.h};
+	MM_CUDA(cudaStreamSynchronize(b->gs));
+	for (size_t k = 0; k < b->slots.size(); ++k) {
+		const mm_batch::Slot &sl = b->slots[k];
+		if (!sl.s) {
+			out_host[k] = mm_batch_result{-1, 0, 0, 0, 0.0, 0.0};
+			continue;
+		}
+		BSlot h{};
+		MM_CUDA(cudaMemcpyAsync(&h, sl.dev, sizeof(BSlot), cudaMemcpyDeviceToHost, st));
+		MM_CUDA(cudaStreamSynchronize(st));
+		out_host[k] = mm_batch_result{h.bs.status, h.bs.steps, h.bs.attempts, h.bs.rejected, h.bs.t, h.bs.h};
 	}
 	return MM_OK;
 }

@@ -25,6 +25,9 @@
 #include <cmath>
 #include <vector>
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace mm {
 
@@ -408,7 +411,7 @@ __host__ __device__ constexpr int ct_lpb(int n, int csize)
 
 // y pass (3-D): TB columns per CTA; forward pads rows n_in -> N, inverse crops N -> n_out.
 // (bx: column tile, plane = c nz + z; shared by the single-grid and the grouped kernels)
-template <typename T, int N, int TB, bool INV>
+template <typename T, int N, int TB, bool INV, int R = ct_radix(N)>
 __device__ __forceinline__ void y_ct_body(cplx<T> *__restrict__ S, int n_in, int n_out, int hx, int lx,
                                           const cplx<T> *__restrict__ twN, int bx, int plane)
 {
@@ -416,7 +419,7 @@ __device__ __forceinline__ void y_ct_body(cplx<T> *__restrict__ S, int n_in, int
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *sm = reinterpret_cast<C *>(smem_raw);
 	const int tid = threadIdx.x;
-	const int line = tid & (TB - 1), j0 = tid / TB;
+	const int line = tid & (TB - 1), j0 = tid / TB;  // N / R threads per column
 	const int kx = bx * TB + line;
 	const bool ok = kx < hx;
 	C *base = S + (size_t)plane * N * lx + (ok ? kx : 0);
@@ -424,7 +427,7 @@ __device__ __forceinline__ void y_ct_body(cplx<T> *__restrict__ S, int n_in, int
 	auto st = [&](int, int k, C v) {
 		if (ok && k < n_out) base[(size_t)k * lx] = v;
 	};
-	cta_fft<T, N, ct_radix(N), TB, INV, SmCols<N, TB>>(sm, twN, line, j0, ld, st);
+	cta_fft<T, N, R, TB, INV, SmCols<N, TB>>(sm, twN, line, j0, ld, st);
 }
 
 template <typename T, int N, int TB, bool INV>
@@ -435,13 +438,13 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__r
 }
 
 // x pass forward: LPB complex lines per CTA (line q packs real rows 2q, 2q+1).
-template <typename T, int N, int LPB, bool SCALE>
+template <typename T, int N, int LPB, bool SCALE, int R = ct_radix(N)>
 __device__ __forceinline__ void x_fwd_ct_body(const T *__restrict__ M, const uint8_t *__restrict__ reg,
                                               const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny,
                                               int nz, int py, int hx, int lx, const cplx<T> *__restrict__ twN, int blk)
 {
 	using C = cplx<T>;
-	constexpr int TPL = N / ct_radix(N);
+	constexpr int TPL = N / R;
 	using SI = SmRows<N, LPB>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *sm = reinterpret_cast<C *>(smem_raw);
@@ -463,7 +466,7 @@ __device__ __forceinline__ void x_fwd_ct_body(const T *__restrict__ M, const uin
 		return C{a, b};
 	};
 	auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
-	cta_fft<T, N, ct_radix(N), LPB, false, SI>(sm, twN, line, j0, ld, st);
+	cta_fft<T, N, R, LPB, false, SI>(sm, twN, line, j0, ld, st);
 	__syncthreads();
 	C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
 	C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
@@ -486,12 +489,12 @@ __global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_ct(const T *_
 }
 
 // x pass inverse: half spectra of rows 2q, 2q+1 -> real rows.
-template <typename T, int N, int LPB>
+template <typename T, int N, int LPB, int R = ct_radix(N)>
 __device__ __forceinline__ void x_inv_ct_body(const cplx<T> *__restrict__ S, T *__restrict__ H, int nx, int ny,
                                               int nz, int py, int hx, int lx, const cplx<T> *__restrict__ twN, int blk)
 {
 	using C = cplx<T>;
-	constexpr int TPL = N / ct_radix(N);
+	constexpr int TPL = N / R;
 	using SI = SmRows<N, LPB>;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *sm = reinterpret_cast<C *>(smem_raw);
@@ -519,7 +522,7 @@ __device__ __forceinline__ void x_inv_ct_body(const cplx<T> *__restrict__ S, T *
 			if (vb) Hb[x] = v.y;
 		}
 	};
-	cta_fft<T, N, ct_radix(N), LPB, true, SI>(sm, twN, line, j0, ld, st);
+	cta_fft<T, N, R, LPB, true, SI>(sm, twN, line, j0, ld, st);
 }
 
 template <typename T, int N, int LPB>
@@ -1578,42 +1581,56 @@ struct GDesc {
 	int nx, ny, nz, py, hx, lx, qy, qz;
 };
 
+// Tile-shape variants the autotuner chooses from per pass and length: 0 the default (radix 16,
+// the single-instance tile), 1 half the lines/columns per CTA, 2 radix-8 passes.
+constexpr int GRP_VARIANTS = 3;
+__host__ __device__ constexpr int var_radix(int n, int v) { return v == 2 ? (n < 8 ? n : 8) : ct_radix(n); }
+__host__ __device__ constexpr int var_tb(int n, int csize, int v)
+{
+	return v == 1 ? (ct_tb(n, csize) > 1 ? ct_tb(n, csize) / 2 : 1) : ct_tb(n, csize);
+}
+__host__ __device__ constexpr int var_lpb(int n, int csize, int v)
+{
+	return v == 1 ? (ct_lpb(n, csize) > 1 ? ct_lpb(n, csize) / 2 : 1) : ct_lpb(n, csize);
+}
+
 __device__ __forceinline__ bool member_skips(const int *flags, int gate)
 {
 	return flags && (!flags[0] || (gate && !flags[1]));
 }
 
-template <typename T, int N, int LPB>
-__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_fwd_grp(const GDesc<T> *__restrict__ d,
+template <typename T, int N, int LPB, int R>
+__global__ void __launch_bounds__(LPB * (N / R)) k_x_fwd_grp(const GDesc<T> *__restrict__ d,
                                                                       const int2 *__restrict__ items, int input,
                                                                       int gate)
 {
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
-	x_fwd_ct_body<T, N, LPB, true>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x,
-	                               it.y);
+	x_fwd_ct_body<T, N, LPB, true, R>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx,
+	                                  g.tw_x, it.y);
 }
 
-template <typename T, int N, int LPB>
-__global__ void __launch_bounds__(LPB * (N / ct_radix(N))) k_x_inv_grp(const GDesc<T> *__restrict__ d,
+template <typename T, int N, int LPB, int R>
+__global__ void __launch_bounds__(LPB * (N / R)) k_x_inv_grp(const GDesc<T> *__restrict__ d,
                                                                       const int2 *__restrict__ items, int gate)
 {
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
-	x_inv_ct_body<T, N, LPB>(g.spec, g.H, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
+	x_inv_ct_body<T, N, LPB, R>(g.spec, g.H, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
 }
 
-template <typename T, int N, int TB, bool INV>
-__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_grp(const GDesc<T> *__restrict__ d,
+template <typename T, int N, int TB, bool INV, int R>
+__global__ void __launch_bounds__(TB * (N / R)) k_y_grp(const GDesc<T> *__restrict__ d,
                                                                     const int2 *__restrict__ items, int gate)
 {
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
 	const int tiles = (g.hx + TB - 1) / TB;
-	y_ct_body<T, N, TB, INV>(g.spec, INV ? N : g.ny, INV ? g.ny : N, g.hx, g.lx, g.tw_y, it.y % tiles, it.y / tiles);
+	y_ct_body<T, N, TB, INV, R>(g.spec, INV ? N : g.ny, INV ? g.ny : N, g.hx, g.lx, g.tw_y, it.y % tiles,
+	                            it.y / tiles);
 }
 
 template <typename T, int PZ>
@@ -1634,8 +1651,9 @@ struct ConvGroup {
 	int count = 0;
 	void *desc = nullptr;  // GDesc<T>[count]
 	struct List {
-		int pass;  // 0 x forward, 1 y forward, 2 z, 3 y inverse, 4 x inverse
-		int len;   // transform length of the pass
+		int pass;     // 0 x forward, 1 y forward, 2 z, 3 y inverse, 4 x inverse
+		int len;      // transform length of the pass
+		int variant;  // tile shape chosen by the autotuner (GRP_VARIANTS)
 		int2 *items;
 		int n;
 	};
@@ -1649,82 +1667,189 @@ struct ConvGroup {
 
 namespace {
 
+// Calls f(std::integral_constant<int, N>, std::integral_constant<int, V>) for a length and a
+// variant; variants other than 0 exist for lengths 16..512.
+template <typename T, class F>
+void with_len_variant(int len, int v, F &&f)
+{
+	auto go = [&](auto nc) {
+		constexpr int N = decltype(nc)::value;
+		if constexpr (N >= 16 && N <= 512) {
+			if (v == 1) { f(nc, std::integral_constant<int, 1>()); return; }
+			if (v == 2) { f(nc, std::integral_constant<int, 2>()); return; }
+		}
+		f(nc, std::integral_constant<int, 0>());
+	};
+#define MM_WLV(N) go(std::integral_constant<int, N>())
+	MM_FS_SWITCH(len, MM_WLV);
+#undef MM_WLV
+}
+
+// Threads of one CTA of a pass/length/variant (0 when the variant does not exist).
 template <typename T>
-mm_status group_smem(int pass, int len)
+int group_threads(int pass, int len, int v)
+{
+	using C = cplx<T>;
+	if (pass == 2) return v == 0 ? ZR_THREADS : 0;
+	if (v != 0 && (len < 16 || len > 512)) return 0;
+	const int csz = (int)sizeof(C);
+	const int lines = (pass == 0 || pass == 4) ? var_lpb(len, csz, v) : var_tb(len, csz, v);
+	if (v == 1 && lines == ((pass == 0 || pass == 4) ? ct_lpb(len, csz) : ct_tb(len, csz))) return 0;
+	const int t = lines * (len / var_radix(len, v));
+	return (t >= 32 && t <= 1024 && (v != 2 || var_radix(len, v) != ct_radix(len))) ? t : 0;
+}
+
+// Blocks of one member for a pass/length/variant.
+template <typename T>
+int group_blocks(const ConvPlan *p, int pass, int len, int v)
+{
+	const int csz = (int)sizeof(cplx<T>);
+	if (pass == 0 || pass == 4) {
+		const int lpb = var_lpb(len, csz, v);
+		return ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
+	}
+	if (pass == 1 || pass == 3) {
+		const int tb = var_tb(len, csz, v);
+		return (p->hx + tb - 1) / tb * 3 * p->nz;
+	}
+	return (p->hx + 31) / 32 * p->qy;
+}
+
+template <typename T>
+size_t group_smem_bytes(int pass, int len, int v)
+{
+	using C = cplx<T>;
+	size_t r = 0;
+	if (pass == 2) return (size_t)2 * len * 96 * sizeof(C);
+	with_len_variant<T>(len, v, [&](auto nc, auto vc) {
+		constexpr int N = decltype(nc)::value, V = decltype(vc)::value;
+		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V);
+		r = (pass == 0 || pass == 4) ? (size_t)SmRows<N, LPB>::SIZE * sizeof(C) : (size_t)SmCols<N, TB>::SIZE * sizeof(C);
+	});
+	return r;
+}
+
+template <typename T>
+mm_status group_smem(int pass, int len, int v)
 {
 	using C = cplx<T>;
 	mm_status r = MM_OK;
-	auto xs = [&](auto nc) {
-		constexpr int N = decltype(nc)::value;
-		constexpr int LPB = ct_lpb(N, sizeof(C)), TB = ct_tb(N, sizeof(C));
-		const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
-		if (pass == 0) r = set_smem<T>((const void *)k_x_fwd_grp<T, N, LPB>, sx);
-		if (pass == 4) r = set_smem<T>((const void *)k_x_inv_grp<T, N, LPB>, sx);
-		if (pass == 1) r = set_smem<T>((const void *)k_y_grp<T, N, TB, false>, sy);
-		if (pass == 3) r = set_smem<T>((const void *)k_y_grp<T, N, TB, true>, sy);
-	};
+	const size_t sm = group_smem_bytes<T>(pass, len, v);
 	if (pass == 2) {
-		const size_t sz = (size_t)2 * len * 96 * sizeof(C);
 		switch (len) {
-		case 2: r = set_smem<T>((const void *)k_z_grp<T, 2>, sz); break;
-		case 4: r = set_smem<T>((const void *)k_z_grp<T, 4>, sz); break;
-		case 8: r = set_smem<T>((const void *)k_z_grp<T, 8>, sz); break;
-		case 16: r = set_smem<T>((const void *)k_z_grp<T, 16>, sz); break;
-		case 32: if constexpr (sizeof(T) == 4) { r = set_smem<T>((const void *)k_z_grp<T, 32>, sz); } break;
+		case 2: r = set_smem<T>((const void *)k_z_grp<T, 2>, sm); break;
+		case 4: r = set_smem<T>((const void *)k_z_grp<T, 4>, sm); break;
+		case 8: r = set_smem<T>((const void *)k_z_grp<T, 8>, sm); break;
+		case 16: r = set_smem<T>((const void *)k_z_grp<T, 16>, sm); break;
+		case 32: if constexpr (sizeof(T) == 4) { r = set_smem<T>((const void *)k_z_grp<T, 32>, sm); } break;
 		}
 		return r;
 	}
-#define MM_GS(N) xs(std::integral_constant<int, N>())
-	MM_FS_SWITCH(len, MM_GS);
-#undef MM_GS
+	with_len_variant<T>(len, v, [&](auto nc, auto vc) {
+		constexpr int N = decltype(nc)::value, V = decltype(vc)::value;
+		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V), R = var_radix(N, V);
+		if (pass == 0) r = set_smem<T>((const void *)k_x_fwd_grp<T, N, LPB, R>, sm);
+		if (pass == 4) r = set_smem<T>((const void *)k_x_inv_grp<T, N, LPB, R>, sm);
+		if (pass == 1) r = set_smem<T>((const void *)k_y_grp<T, N, TB, false, R>, sm);
+		if (pass == 3) r = set_smem<T>((const void *)k_y_grp<T, N, TB, true, R>, sm);
+	});
 	return r;
+}
+
+template <typename T>
+void group_launch_v(const GDesc<T> *d, int pass, int len, int v, const int2 *items, int n, int input, int gate,
+                    cudaStream_t st)
+{
+	using C = cplx<T>;
+	const size_t sm = group_smem_bytes<T>(pass, len, v);
+	if (pass == 2) {
+		switch (len) {
+		case 2: k_z_grp<T, 2><<<n, ZR_THREADS, sm, st>>>(d, items, gate); break;
+		case 4: k_z_grp<T, 4><<<n, ZR_THREADS, sm, st>>>(d, items, gate); break;
+		case 8: k_z_grp<T, 8><<<n, ZR_THREADS, sm, st>>>(d, items, gate); break;
+		case 16: k_z_grp<T, 16><<<n, ZR_THREADS, sm, st>>>(d, items, gate); break;
+		case 32: if constexpr (sizeof(T) == 4) { k_z_grp<T, 32><<<n, ZR_THREADS, sm, st>>>(d, items, gate); } break;
+		}
+		return;
+	}
+	with_len_variant<T>(len, v, [&](auto nc, auto vc) {
+		constexpr int N = decltype(nc)::value, V = decltype(vc)::value;
+		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V), R = var_radix(N, V);
+		constexpr int TPL = N / R;
+		if (pass == 0) k_x_fwd_grp<T, N, LPB, R><<<n, LPB * TPL, sm, st>>>(d, items, input, gate);
+		if (pass == 4) k_x_inv_grp<T, N, LPB, R><<<n, LPB * TPL, sm, st>>>(d, items, gate);
+		if (pass == 1) k_y_grp<T, N, TB, false, R><<<n, TB * TPL, sm, st>>>(d, items, gate);
+		if (pass == 3) k_y_grp<T, N, TB, true, R><<<n, TB * TPL, sm, st>>>(d, items, gate);
+	});
 }
 
 template <typename T>
 void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, int gate, cudaStream_t st)
 {
-	using C = cplx<T>;
-	const GDesc<T> *d = (const GDesc<T> *)g->desc;
-	auto xs = [&](auto nc) {
-		constexpr int N = decltype(nc)::value;
-		constexpr int LPB = ct_lpb(N, sizeof(C)), TB = ct_tb(N, sizeof(C)), TPL = N / ct_radix(N);
-		const size_t sx = (size_t)SmRows<N, LPB>::SIZE * sizeof(C), sy = (size_t)SmCols<N, TB>::SIZE * sizeof(C);
-		if (l.pass == 0) k_x_fwd_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, input, gate);
-		if (l.pass == 4) k_x_inv_grp<T, N, LPB><<<l.n, LPB * TPL, sx, st>>>(d, l.items, gate);
-		if (l.pass == 1) k_y_grp<T, N, TB, false><<<l.n, TB * TPL, sy, st>>>(d, l.items, gate);
-		if (l.pass == 3) k_y_grp<T, N, TB, true><<<l.n, TB * TPL, sy, st>>>(d, l.items, gate);
-	};
-	if (l.pass == 2) {
-		const size_t sz = (size_t)2 * l.len * 96 * sizeof(C);
-		switch (l.len) {
-		case 2: k_z_grp<T, 2><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
-		case 4: k_z_grp<T, 4><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
-		case 8: k_z_grp<T, 8><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
-		case 16: k_z_grp<T, 16><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); break;
-		case 32: if constexpr (sizeof(T) == 4) { k_z_grp<T, 32><<<l.n, ZR_THREADS, sz, st>>>(d, l.items, gate); } break;
-		}
-		return;
+	group_launch_v<T>((const GDesc<T> *)g->desc, l.pass, l.len, l.variant, l.items, l.n, input, gate, st);
+}
+
+// The autotuner's choices, per precision, pass and length, for the process (tuned once, on the
+// first group that uses a pass and length, by timing every variant on that group's members).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tuned;
+
+template <typename T>
+std::vector<int2> group_items(const ConvGroupMember *m, const std::vector<int> &mem, int pass, int len, int v)
+{
+	std::vector<int2> items;
+	for (int i : mem) {
+		const int nb = group_blocks<T>(m[i].plan, pass, len, v);
+		for (int b = 0; b < nb; ++b) items.push_back(make_int2(i, b));
 	}
-#define MM_GL(N) xs(std::integral_constant<int, N>())
-	MM_FS_SWITCH(l.len, MM_GL);
-#undef MM_GL
+	return items;
+}
+
+// Times every variant of one pass and length on the group's members (run flags ignored) and
+// returns the fastest.
+template <typename T>
+mm_status group_tune(const GDesc<T> *d, const ConvGroupMember *m, const std::vector<int> &mem, int pass, int len,
+                     cudaStream_t st, int *best)
+{
+	*best = 0;
+	float best_ms = 0.f;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	MM_CUDA(cudaEventCreate(&e0));
+	MM_CUDA(cudaEventCreate(&e1));
+	mm_status r = MM_OK;
+	for (int v = 0; v < GRP_VARIANTS && r == MM_OK; ++v) {
+		if (!group_threads<T>(pass, len, v) || group_smem_bytes<T>(pass, len, v) > 227 * 1024) continue;
+		const std::vector<int2> items = group_items<T>(m, mem, pass, len, v);
+		int2 *di = nullptr;
+		r = cuda_status(cudaMalloc(&di, sizeof(int2) * items.size()), "cudaMalloc");
+		if (r == MM_OK) r = cuda_status(cudaMemcpyAsync(di, items.data(), sizeof(int2) * items.size(),
+		                                                cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
+		if (r == MM_OK) r = group_smem<T>(pass, len, v);
+		if (r == MM_OK) {
+			group_launch_v<T>(d, pass, len, v, di, (int)items.size(), 0, 0, st);  // warm-up
+			cudaEventRecord(e0, st);
+			for (int k = 0; k < 3; ++k) group_launch_v<T>(d, pass, len, v, di, (int)items.size(), 0, 0, st);
+			cudaEventRecord(e1, st);
+			r = cuda_status(cudaEventSynchronize(e1), "autotune launch");
+		}
+		float ms = 0.f;
+		if (r == MM_OK) r = cuda_status(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+		if (r == MM_OK && (v == 0 || ms < best_ms)) {
+			best_ms = ms;
+			*best = v;
+		}
+		cudaFree(di);
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	return r;
 }
 
 template <typename T>
 mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaStream_t st)
 {
 	std::vector<GDesc<T>> h(count);
-	std::vector<std::vector<int2>> items[5];
-	std::vector<int> lens[5];
-	auto add = [&](int pass, int len, int member, int blocks) {
-		size_t k = 0;
-		while (k < lens[pass].size() && lens[pass][k] != len) ++k;
-		if (k == lens[pass].size()) {
-			lens[pass].push_back(len);
-			items[pass].emplace_back();
-		}
-		for (int b = 0; b < blocks; ++b) items[pass][k].push_back(make_int2(member, b));
-	};
+	std::map<std::pair<int, int>, std::vector<int>> lists;  // (pass, length) -> members
 	for (int i = 0; i < count; ++i) {
 		const ConvPlan *p = m[i].plan;
 		if (!p || p->prec != g->prec || p->is2d || !p->fast_x || !p->fast_y || !p->reg_z)
@@ -1738,37 +1863,43 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		d.H = (T *)m[i].H;
 		d.reg = m[i].reg;
 		d.ms_tab = (const T *)m[i].ms_tab;
-		d.flags = m[i].flags;
+		d.flags = nullptr;  // the autotuner runs every member; the real flags are set below
 		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
 		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
-		using C = cplx<T>;
-		int lpb = 1, tb = 1;
-#define MM_GEO(N) (lpb = ct_lpb(N, sizeof(C)), tb = ct_tb(N, sizeof(C)))
-		MM_FS_SWITCH(p->px, MM_GEO);
-		const int xblocks = ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
-		switch (p->py) {
-		case 4: MM_GEO(4); break; case 8: MM_GEO(8); break; case 16: MM_GEO(16); break; case 32: MM_GEO(32); break;
-		case 64: MM_GEO(64); break; case 128: MM_GEO(128); break; case 256: MM_GEO(256); break;
-		case 512: MM_GEO(512); break; case 1024: MM_GEO(1024); break;
-		case 2048: if constexpr (sizeof(T) == 4) { MM_GEO(2048); } break;
-		}
-#undef MM_GEO
-		add(0, p->px, i, xblocks);
-		add(1, p->py, i, (p->hx + tb - 1) / tb * 3 * p->nz);
-		add(2, p->pz, i, (p->hx + 31) / 32 * p->qy);
-		add(3, p->py, i, (p->hx + tb - 1) / tb * 3 * p->nz);
-		add(4, p->px, i, xblocks);
+		lists[{0, p->px}].push_back(i);
+		lists[{1, p->py}].push_back(i);
+		lists[{2, p->pz}].push_back(i);
+		lists[{3, p->py}].push_back(i);
+		lists[{4, p->px}].push_back(i);
 	}
 	MM_CUDA(cudaMalloc(&g->desc, sizeof(GDesc<T>) * count));
 	MM_CUDA(cudaMemcpyAsync(g->desc, h.data(), sizeof(GDesc<T>) * count, cudaMemcpyHostToDevice, st));
-	for (int pass = 0; pass < 5; ++pass)
-		for (size_t k = 0; k < lens[pass].size(); ++k) {
-			ConvGroup::List l{pass, lens[pass][k], nullptr, (int)items[pass][k].size()};
-			MM_CUDA(cudaMalloc(&l.items, sizeof(int2) * l.n));
-			MM_CUDA(cudaMemcpyAsync(l.items, items[pass][k].data(), sizeof(int2) * l.n, cudaMemcpyHostToDevice, st));
-			g->lists.push_back(l);
-			MM_TRY(group_smem<T>(pass, l.len));
+	for (const auto &kv : lists) {
+		const int pass = kv.first.first, len = kv.first.second;
+		int v = 0;
+		bool known = false;
+		{
+			std::lock_guard<std::mutex> lock(g_tune_mu);
+			auto it = g_tuned.find(std::make_tuple(g->prec, pass, len));
+			if (it != g_tuned.end()) { v = it->second; known = true; }
 		}
+		if (!known) {
+			MM_TRY(group_tune<T>((const GDesc<T> *)g->desc, m, kv.second, pass, len, st, &v));
+			std::lock_guard<std::mutex> lock(g_tune_mu);
+			g_tuned[std::make_tuple(g->prec, pass, len)] = v;
+		}
+		const std::vector<int2> items = group_items<T>(m, kv.second, pass, len, v);
+		ConvGroup::List l{pass, len, v, nullptr, (int)items.size()};
+		MM_CUDA(cudaMalloc(&l.items, sizeof(int2) * l.n));
+		MM_CUDA(cudaMemcpyAsync(l.items, items.data(), sizeof(int2) * l.n, cudaMemcpyHostToDevice, st));
+		MM_TRY(group_smem<T>(pass, len, v));
+		g->lists.push_back(l);
+	}
+	// lists in pass order (x forward, y forward, z, y inverse, x inverse)
+	std::stable_sort(g->lists.begin(), g->lists.end(),
+	                 [](const ConvGroup::List &a, const ConvGroup::List &b) { return a.pass < b.pass; });
+	for (int i = 0; i < count; ++i) h[i].flags = m[i].flags;
+	MM_CUDA(cudaMemcpyAsync(g->desc, h.data(), sizeof(GDesc<T>) * count, cudaMemcpyHostToDevice, st));
 	MM_CUDA(cudaStreamSynchronize(st));
 	return MM_OK;
 }

@@ -29,6 +29,7 @@
 #include <vector>
 #include <cstring>
 #include <cmath>
+#include <utility>
 
 namespace mm {
 
@@ -286,13 +287,35 @@ constexpr int stage_min_blocks() { return sizeof(T) == 4 ? 3 : 2; }  // FP64 nee
 
 // One tile (32*STAGE_CPT x 8 cells of plane z) of the fused stage; the maxima of the error, of
 // |k_0| and (TORQUE) of |m x H_eff| / Ms accumulate in e2, k02, tq2.
+// Asynchronous element copy global -> shared (LDGSTS), finished by cp_async_wait_all().
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T *dst, const T *src)
+{
+	const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+	if constexpr (sizeof(T) == 4)
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+	else
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Prefetch slots per cell of a stage tile: y_n (3), its compensation (3), k_0..k_{MAXS-2} (3 each).
+constexpr int STAGE_PRE = 6 + 3 * (MAXS - 1);
+template <typename T>
+constexpr size_t stage_smem() { return (size_t)STAGE_PRE * STAGE_CPT * 256 * sizeof(T); }
+
+// One tile (32*STAGE_CPT x 8 cells of plane z) of the fused stage; the maxima of the error, of
+// |k_0| and (TORQUE) of |m x H_eff| / Ms accumulate in e2, k02, tq2.  The operands of the stage
+// combination (y_n, its compensation, the earlier stage vectors with nonzero weight) are copied
+// into shared memory asynchronously while the field and k_i are computed; `pre` is the block's
+// STAGE_PRE * STAGE_CPT * 256 slots.
 template <typename T, bool COMP, int S, bool TORQUE>
 __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__restrict__ msr, const StageCoef &sc,
                                            const T *__restrict__ y_in, const T *__restrict__ Hd,
                                            const T *__restrict__ yhi, const T *__restrict__ ylo, T *const *K,
                                            T *__restrict__ y_out, T *__restrict__ y_out_lo,
                                            const DevState *__restrict__ st, int tile, int tiles_x, int tiles_y,
-                                           T &e2, T &k02, T &tq2)
+                                           T &e2, T &k02, T &tq2, T *pre)
 {
 	const size_t n = (size_t)a.nx * a.ny * a.nz;
 	const double h = st->h;
@@ -300,14 +323,38 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 	const int yy = (rest % tiles_y) * blockDim.y + threadIdx.y;
 	const int z = rest / tiles_y;
 	const double t = st->t + sc.a_i * h;
+	const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+	auto slot = [&](int u, int k) -> T & { return pre[(u * STAGE_PRE + k) * 256 + tid]; };
+	auto pre3 = [&](int u, int k) { return v3<T>(slot(u, k), slot(u, k + 1), slot(u, k + 2)); };
 	V3<T> ki[STAGE_CPT];
 	size_t idx[STAGE_CPT];
 	bool in[STAGE_CPT];
+	// which operands the combination needs (uniform over the block)
+	const bool out = sc.last ? sc.write_new : sc.write_next;
+	bool needk[MAXS];
+#pragma unroll
+	for (int l = 0; l < MAXS; ++l)
+		needk[l] = l < S && (sc.last ? (sc.ec[l] != 0.0 || (sc.write_new && sc.bn[l] != 0.0))
+		                             : ((sc.write_next && sc.bn[l] != 0.0) || (sc.reduce_k0 && l == 0)));
 #pragma unroll
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
 		in[u] = x < a.nx && yy < a.ny;
 		idx[u] = ((size_t)z * a.ny + (in[u] ? yy : 0)) * a.nx + (in[u] ? x : 0);
+		if (in[u]) {
+			for (int c = 0; c < 3; ++c) {
+				const size_t e = idx[u] + c * n;
+				if (out) cp_async_elem(&slot(u, c), yhi + e);
+				if (out && COMP) cp_async_elem(&slot(u, 3 + c), ylo + e);
+#pragma unroll
+				for (int l = 0; l < S; ++l)
+					if (needk[l]) cp_async_elem(&slot(u, 6 + 3 * l + c), K[l] + e);
+			}
+		}
+	}
+#pragma unroll
+	for (int u = 0; u < STAGE_CPT; ++u) {
+		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
 		if (in[u]) {
 			V3<T> Heff;
 			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
@@ -321,24 +368,25 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 			}
 		}
 	}
+	cp_async_wait_all();
 #pragma unroll
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		if (!in[u]) continue;
 		const size_t i = idx[u];
 		if (!sc.last) {
 			if (sc.write_next) {
-				V3<T> acc = COMP ? load3(ylo, i, n) : load3(yhi, i, n);
+				V3<T> acc = COMP ? pre3(u, 3) : pre3(u, 0);
 #pragma unroll
 				for (int l = 0; l < S; ++l) {
 					const T f = (T)(h * sc.bn[l]);
-					if (f != T(0)) acc = acc + f * load3(K[l], i, n);
+					if (f != T(0)) acc = acc + f * pre3(u, 6 + 3 * l);
 				}
 				acc = acc + (T)(h * sc.bn[S]) * ki[u];
-				if (COMP) acc = load3(yhi, i, n) + acc;
+				if (COMP) acc = pre3(u, 0) + acc;
 				store3(y_out, i, n, acc);
 			}
 			if (sc.reduce_k0) {
-				const V3<T> k0 = S == 0 ? ki[u] : load3(K[0], i, n);
+				const V3<T> k0 = S == 0 ? ki[u] : pre3(u, 6);
 				k02 = max(k02, dot(k0, k0));
 			}
 		} else {
@@ -349,7 +397,7 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 				const T fe = (T)(h * sc.ec[l]);
 				const T fc = (T)(h * sc.bn[l]);
 				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
-				const V3<T> kl = l == S ? ki[u] : load3(K[l], i, n);
+				const V3<T> kl = l == S ? ki[u] : pre3(u, 6 + 3 * l);
 				err = err + fe * kl;
 				if (sc.write_new) acc = acc + fc * kl;
 			}
@@ -357,15 +405,15 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 			if (sc.write_new) {
 				if (COMP) {
 					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
-					const V3<T> hi = load3(yhi, i, n);
-					const V3<T> d = load3(ylo, i, n) + acc;
+					const V3<T> hi = pre3(u, 0);
+					const V3<T> d = pre3(u, 3) + acc;
 					const V3<T> s = hi + d;
 					const V3<T> bb = s - hi;
 					const V3<T> lo = (hi - (s - bb)) + (d - bb);
 					store3(y_out, i, n, s);
 					store3(y_out_lo, i, n, lo);
 				} else {
-					store3(y_out, i, n, load3(yhi, i, n) + acc);
+					store3(y_out, i, n, pre3(u, 0) + acc);
 				}
 			}
 		}
@@ -381,12 +429,13 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
             double *red_k0, int tiles_x, int tiles_y, int ntiles)
 {
 	__shared__ T msr[256];
+	extern __shared__ __align__(16) unsigned char stage_pre[];
 	load_ms_table(a, msr);
 	T *const *K = ktab->k;
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
 	for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
 		stage_tile<T, COMP, S, false>(a, msr, sc, y_in, Hd, yhi, ylo, K, y_out, y_out_lo, st, tile, tiles_x, tiles_y,
-		                              e2, k02, tq2);
+		                              e2, k02, tq2, reinterpret_cast<T *>(stage_pre));
 	if (sc.last) block_max_to(red_err, e2);
 	if (sc.reduce_k0) block_max_to(red_k0, k02);
 }
@@ -786,12 +835,21 @@ double stage_bytes(const mm_solver *s, const StageCoef &sc)
 
 // Resident blocks of the fused stage kernel on the whole device (occupancy of the S = 6 instance),
 // looked up once; solver creation calls it so that no later call does so during stream capture.
+template <typename T, bool COMP, int... S>
+void stage_smem_attrs(std::integer_sequence<int, S...>)
+{
+	const int bytes = (int)stage_smem<T>();
+	(cudaFuncSetAttribute(k_stage<T, COMP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
+}
+
 template <typename T, bool COMP>
 int stage_resident()
 {
 	static const int resident = [] {
+		stage_smem_attrs<T, COMP>(std::make_integer_sequence<int, MAXS>());
 		int per_sm = 0;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<T, COMP, 6>, 256, 0) != cudaSuccess ||
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<T, COMP, 6>, 256, stage_smem<T>()) !=
+		        cudaSuccess ||
 		    per_sm < 1) {
 			cudaGetLastError();
 			per_sm = stage_min_blocks<T>();
@@ -810,7 +868,7 @@ void stage_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc,
 	const dim3 tg = stage_grid(s->cfg);
 	const int ntiles = (int)(tg.x * tg.y * tg.z);
 	const int grid = ntiles < resident ? ntiles : resident;
-	k_stage<T, COMP, S><<<grid, dim3(32, 8, 1), 0, st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, yout,
+	k_stage<T, COMP, S><<<grid, dim3(32, 8, 1), stage_smem<T>(), st>>>(a, sc, yin, (const T *)s->hd, yhi, ylo, kt, yout,
 	                                                     (T *)s->ynew_lo, ds, &ds->max_err2, &ds->max_k02,
 	                                                     (int)tg.x, (int)tg.y, ntiles);
 }
@@ -1473,6 +1531,7 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 	if (!g.slot->active || (S == 0 && !g.slot->need_k0)) return;
 	__shared__ CellArgs<T> a;
 	__shared__ T msr[256];
+	extern __shared__ __align__(16) unsigned char stage_pre[];
 	if (threadIdx.x == 0 && threadIdx.y == 0) a = g.a;
 	__syncthreads();
 	load_ms_table(a, msr);
@@ -1483,7 +1542,7 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
 	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
 		stage_tile<T, COMP, S, TORQUE>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds, it.y + k,
-		                               g.tiles_x, g.tiles_y, e2, k02, tq2);
+		                               g.tiles_x, g.tiles_y, e2, k02, tq2, reinterpret_cast<T *>(stage_pre));
 	if (sc.last) block_max_to(&g.ds->max_err2, e2);
 	if (sc.reduce_k0) block_max_to(&g.ds->max_k02, k02);
 	if (TORQUE) block_max_to(&g.ds->max_tq2, tq2);
@@ -1663,9 +1722,11 @@ void launch_stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, c
 {
 	const BDesc<T> *d = (const BDesc<T> *)b->desc;
 	if (sc.last)
-		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items);
+		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
+		                                                                               b->stage_items);
 	else
-		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), 0, st>>>(d, sc, in, out, b->stage_items);
+		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
+		                                                                                b->stage_items);
 }
 
 template <typename T, bool COMP>
@@ -1735,6 +1796,14 @@ mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 	k_accept_grp<T, COMP><<<b->n_cell, 256, 0, st>>>(d, last_buf, b->cell_items);
 	MM_TRY(after_launch("k_accept_grp"));
 	return MM_OK;
+}
+
+template <typename T, bool COMP, int... S>
+void stage_grp_attrs(std::integer_sequence<int, S...>)
+{
+	const int bytes = (int)stage_smem<T>();
+	(cudaFuncSetAttribute(k_stage_grp<T, COMP, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
+	(cudaFuncSetAttribute(k_stage_grp<T, COMP, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
 }
 
 // Captures one round into a graph on the batch's private stream.
@@ -1812,6 +1881,7 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 	b->n_cell3 = (int)c3.size();
 	b->n_cell = (int)c1.size();
 	MM_CUDA(cudaStreamSynchronize(st));
+	stage_grp_attrs<T, sizeof(T) == 4>(std::make_integer_sequence<int, 7>());
 	MM_TRY(batch_graph<T>(b, 0));
 	MM_TRY(batch_graph<T>(b, 1));
 	return MM_OK;

@@ -1,7 +1,8 @@
 """GPU tests of the batched relaxations: every instance of a batch follows the same trajectory as
-the single-instance solver with the same geometry and controller (3-D instances take the same
-power-of-two passes there), an instance's result does not depend on the batch around it, and the
-torque stop criterion holds at the returned states (checked by the FP64 oracle)."""
+the single-instance solver with the same geometry and controller (within the FP32 tolerance: the
+autotuned grouped passes may factor the FFTs differently), an instance's result does not depend on
+the batch around it (bit for bit), and the torque stop criterion holds at the returned states
+(checked by the FP64 oracle)."""
 import numpy as np
 import pytest
 import torch
@@ -72,7 +73,10 @@ def test_batch_instances_follow_the_single_solver(bt, sv):
         assert s.stats["steps"] == r["steps"]
         got, ref = b.get_M(i), s.M
         err = float((got - ref).abs().max()) / q.Ms
-        assert err < 1e-6, (i, err)
+        # same step sequence; the autotuner may pick another FFT factorisation for the grouped
+        # passes than the single-instance passes use, so the FP32 rounding differs: the FP32
+        # trajectory tolerance applies
+        assert err < 1e-4, (i, err)
         assert s.stats["t"] == pytest.approx(r["t"], rel=1e-12)
 
 

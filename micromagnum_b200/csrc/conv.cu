@@ -23,6 +23,7 @@
 #include "tma.cuh"
 
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 #include <algorithm>
 #include <map>
@@ -1882,6 +1883,12 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 			std::lock_guard<std::mutex> lock(g_tune_mu);
 			auto it = g_tuned.find(std::make_tuple(g->prec, pass, len));
 			if (it != g_tuned.end()) { v = it->second; known = true; }
+		}
+		// MMB200_GROUP_VARIANT=0|1|2 fixes the variant (where it exists) instead of timing them
+		if (const char *fv = std::getenv("MMB200_GROUP_VARIANT")) {
+			const int f = std::atoi(fv);
+			v = (f >= 0 && f < GRP_VARIANTS && group_threads<T>(pass, len, f)) ? f : 0;
+			known = true;
 		}
 		if (!known) {
 			MM_TRY(group_tune<T>((const GDesc<T> *)g->desc, m, kv.second, pass, len, st, &v));

@@ -1583,8 +1583,9 @@ struct GDesc {
 };
 
 // Tile-shape variants the autotuner chooses from per pass and length: 0 the default (radix 16,
-// the single-instance tile), 1 half the lines/columns per CTA, 2 radix-8 passes.
-constexpr int GRP_VARIANTS = 3;
+// the single-instance tile), 1 half the lines/columns per CTA, 2 radix-8 passes, 3 (y passes
+// only) TMA-staged tiles on persistent CTAs.
+constexpr int GRP_VARIANTS = 4;
 __host__ __device__ constexpr int var_radix(int n, int v) { return v == 2 ? (n < 8 ? n : 8) : ct_radix(n); }
 __host__ __device__ constexpr int var_tb(int n, int csize, int v)
 {
@@ -1645,6 +1646,93 @@ __global__ void __launch_bounds__(ZR_THREADS, 3) k_z_grp(const GDesc<T> *__restr
 	z_reg_body<T, PZ>(g.spec, g.tensor, g.nz, g.py, g.hx, g.lx, g.qy, g.qz, it.y % tiles, it.y / tiles);
 }
 
+// Grouped y pass through TMA-staged tiles (the autotuner's variant 3): persistent CTAs walk the
+// work list (member, column tile) of one length, skipping members whose run flags say so; each
+// member has its own tensor maps (maps[2 member + INV], in global memory).  Pipeline as k_y_tma.
+template <typename T, int N, bool INV>
+__global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)), 1)
+    k_y_tma_grp(const GDesc<T> *__restrict__ d, const CUtensorMap *__restrict__ maps, const int2 *__restrict__ items,
+                int n_items, int gate, int *err)
+{
+	using C = cplx<T>;
+	constexpr int TB = ct_tb(N, sizeof(C));
+	using G = YTmaGeom<N, TB, INV, C>;
+	constexpr int R = ct_radix(N);
+	using SI = SmCols<N, TB>;
+	extern __shared__ __align__(128) unsigned char smem_tma[];
+	C *stage0 = reinterpret_cast<C *>(smem_tma);
+	C *stage1 = stage0 + TB * G::ROWS;
+	C *work = reinterpret_cast<C *>(smem_tma + 2 * (size_t)G::TILE_BYTES);
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * (size_t)G::TILE_BYTES + G::WORK);
+	const int tid = threadIdx.x;
+	const int line = tid & (TB - 1), j0 = tid / TB;
+	// this CTA's tiles: t = blockIdx.x + k gridDim.x, members that run only
+	auto next_tile = [&](int t) {
+		while (t < n_items && member_skips(d[items[t].x].flags, gate)) t += gridDim.x;
+		return t;
+	};
+	auto issue = [&](int t, int b) {
+		const int2 it = items[t];
+		const int tiles_x = (d[it.x].hx + TB - 1) / TB;
+		const int tx = it.y % tiles_x, plane = it.y / tiles_x;
+		C *dst = b ? stage1 : stage0;
+		const CUtensorMap *map = &maps[2 * it.x + (INV ? 1 : 0)];
+		// the maps were written by a host copy before the launch: order those writes before the
+		// tensor-map proxy reads them
+		asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+		mbar_expect_tx(&bar[b], G::TILE_BYTES);
+#pragma unroll
+		for (int q = 0; q < G::NBOX; ++q)
+			tma_load_3d(dst + q * G::BR * TB, map, tx * TB * G::E, q * G::BR, plane, &bar[b]);
+	};
+	if (tid == 0) {
+		mbar_init(&bar[0], 1);
+		mbar_init(&bar[1], 1);
+		fence_proxy_async();
+	}
+	__syncthreads();
+	int t = next_tile(blockIdx.x);
+	int t1 = t < n_items ? next_tile(t + gridDim.x) : n_items;
+	if (tid == 0) {
+		if (t < n_items) issue(t, 0);
+		if (t1 < n_items) issue(t1, 1);
+	}
+	uint32_t parity = 0;
+	for (int k = 0; t < n_items; ++k) {
+		const int b = k & 1;
+		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+		if (__syncthreads_or(late)) {
+			if (tid == 0) atomicExch(err, 1);
+			return;
+		}
+		parity ^= 1u << b;
+		const int2 it = items[t];
+		const GDesc<T> &g = d[it.x];
+		const int tiles_x = (g.hx + TB - 1) / TB;
+		const int tx = it.y % tiles_x, plane = it.y / tiles_x;
+		const int kx = tx * TB + line;
+		const bool ok = kx < g.hx;
+		const int lx = g.lx, n_out = INV ? g.ny : N;
+		C *base = g.spec + (size_t)plane * N * lx + (ok ? kx : 0);
+		const C *sb = b ? stage1 : stage0;
+		auto ld = [&](int, int r) -> C { return r < G::ROWS ? sb[r * TB + line] : C{0, 0}; };
+		auto st = [&](int, int r, C v) {
+			if (ok && r < n_out) base[(size_t)r * lx] = v;
+		};
+		const int t2 = t1 < n_items ? next_tile(t1 + gridDim.x) : n_items;
+		auto release = [&]() {
+			__syncthreads();  // every thread has read stage buffer b
+			if (tid == 0 && t2 < n_items) {
+				fence_proxy_async();
+				issue(t2, b);
+			}
+		};
+		cta_fft<T, N, R, TB, INV, SI>(work, g.tw_y, line, j0, ld, st, release);
+		t = t1;
+		t1 = t2;
+	}
+}
+
 } // namespace
 
 struct ConvGroup {
@@ -1657,11 +1745,17 @@ struct ConvGroup {
 		int variant;  // tile shape chosen by the autotuner (GRP_VARIANTS)
 		int2 *items;
 		int n;
+		int grid;     // persistent grid of variant 3
 	};
 	std::vector<List> lists;
+	CUtensorMap *maps = nullptr;  // [2 member + inverse]: spectrum views of the y passes
+	bool maps_ok = false;         // every member's maps exist (variant 3 possible)
+	int *err = nullptr;           // set when a staged pass gave up waiting
 	~ConvGroup()
 	{
 		cudaFree(desc);
+		cudaFree(maps);
+		cudaFree(err);
 		for (auto &l : lists) cudaFree(l.items);
 	}
 };
@@ -1692,6 +1786,12 @@ int group_threads(int pass, int len, int v)
 {
 	using C = cplx<T>;
 	if (pass == 2) return v == 0 ? ZR_THREADS : 0;
+	if (v == 3) {
+		if (pass != 1 && pass != 3) return 0;
+		const int tb = ct_tb(len, (int)sizeof(C));
+		if (tb * (int)sizeof(C) < 16 || tb * (int)(sizeof(C) / 8) > 256) return 0;
+		return tb * (len / ct_radix(len));
+	}
 	if (v != 0 && (len < 16 || len > 512)) return 0;
 	const int csz = (int)sizeof(C);
 	const int lines = (pass == 0 || pass == 4) ? var_lpb(len, csz, v) : var_tb(len, csz, v);
@@ -1710,7 +1810,7 @@ int group_blocks(const ConvPlan *p, int pass, int len, int v)
 		return ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
 	}
 	if (pass == 1 || pass == 3) {
-		const int tb = var_tb(len, csz, v);
+		const int tb = var_tb(len, csz, v == 3 ? 0 : v);
 		return (p->hx + tb - 1) / tb * 3 * p->nz;
 	}
 	return (p->hx + 31) / 32 * p->qy;
@@ -1722,6 +1822,16 @@ size_t group_smem_bytes(int pass, int len, int v)
 	using C = cplx<T>;
 	size_t r = 0;
 	if (pass == 2) return (size_t)2 * len * 96 * sizeof(C);
+	if (v == 3) {
+		auto y3 = [&](auto nc) {
+			constexpr int N = decltype(nc)::value, TB = ct_tb(N, sizeof(C));
+			r = pass == 1 ? YTmaGeom<N, TB, false, C>::SMEM : YTmaGeom<N, TB, true, C>::SMEM;
+		};
+#define MM_Y3(N) y3(std::integral_constant<int, N>())
+		MM_FS_SWITCH(len, MM_Y3);
+#undef MM_Y3
+		return r;
+	}
 	with_len_variant<T>(len, v, [&](auto nc, auto vc) {
 		constexpr int N = decltype(nc)::value, V = decltype(vc)::value;
 		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V);
@@ -1746,6 +1856,16 @@ mm_status group_smem(int pass, int len, int v)
 		}
 		return r;
 	}
+	if (v == 3) {
+		auto y3 = [&](auto nc) {
+			constexpr int N = decltype(nc)::value;
+			r = set_smem<T>(pass == 1 ? (const void *)k_y_tma_grp<T, N, false> : (const void *)k_y_tma_grp<T, N, true>, sm);
+		};
+#define MM_Y3(N) y3(std::integral_constant<int, N>())
+		MM_FS_SWITCH(len, MM_Y3);
+#undef MM_Y3
+		return r;
+	}
 	with_len_variant<T>(len, v, [&](auto nc, auto vc) {
 		constexpr int N = decltype(nc)::value, V = decltype(vc)::value;
 		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V), R = var_radix(N, V);
@@ -1758,11 +1878,25 @@ mm_status group_smem(int pass, int len, int v)
 }
 
 template <typename T>
-void group_launch_v(const GDesc<T> *d, int pass, int len, int v, const int2 *items, int n, int input, int gate,
-                    cudaStream_t st)
+void group_launch_v(const ConvGroup *g, int pass, int len, int v, const int2 *items, int n, int grid, int input,
+                    int gate, cudaStream_t st)
 {
 	using C = cplx<T>;
+	const GDesc<T> *d = (const GDesc<T> *)g->desc;
 	const size_t sm = group_smem_bytes<T>(pass, len, v);
+	if (v == 3) {
+		auto y3 = [&](auto nc) {
+			constexpr int N = decltype(nc)::value, TB = ct_tb(N, sizeof(C));
+			const int threads = TB * (N / ct_radix(N));
+			const int gr = grid < n ? grid : n;
+			if (pass == 1) k_y_tma_grp<T, N, false><<<gr, threads, sm, st>>>(d, g->maps, items, n, gate, g->err);
+			else k_y_tma_grp<T, N, true><<<gr, threads, sm, st>>>(d, g->maps, items, n, gate, g->err);
+		};
+#define MM_Y3(N) y3(std::integral_constant<int, N>())
+		MM_FS_SWITCH(len, MM_Y3);
+#undef MM_Y3
+		return;
+	}
 	if (pass == 2) {
 		switch (len) {
 		case 2: k_z_grp<T, 2><<<n, ZR_THREADS, sm, st>>>(d, items, gate); break;
@@ -1787,7 +1921,28 @@ void group_launch_v(const GDesc<T> *d, int pass, int len, int v, const int2 *ite
 template <typename T>
 void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, int gate, cudaStream_t st)
 {
-	group_launch_v<T>((const GDesc<T> *)g->desc, l.pass, l.len, l.variant, l.items, l.n, input, gate, st);
+	group_launch_v<T>(g, l.pass, l.len, l.variant, l.items, l.n, l.grid, input, gate, st);
+}
+
+// Persistent grid of the TMA-staged grouped y pass (resident CTAs on the whole device).
+template <typename T>
+int group_grid(int pass, int len)
+{
+	using C = cplx<T>;
+	int occ = 0;
+	auto y3 = [&](auto nc) {
+		constexpr int N = decltype(nc)::value, TB = ct_tb(N, sizeof(C));
+		const int threads = TB * (N / ct_radix(N));
+		const size_t sm = group_smem_bytes<T>(pass, N, 3);
+		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, pass == 1 ? (const void *)k_y_tma_grp<T, N, false>
+		                                                                  : (const void *)k_y_tma_grp<T, N, true>,
+		                                                  threads, sm) != cudaSuccess)
+			cudaGetLastError();
+	};
+#define MM_Y3(N) y3(std::integral_constant<int, N>())
+	MM_FS_SWITCH(len, MM_Y3);
+#undef MM_Y3
+	return (occ > 0 ? occ : 1) * num_sms();
 }
 
 // The autotuner's choices, per precision, pass and length, for the process (tuned once, on the
@@ -1809,7 +1964,7 @@ std::vector<int2> group_items(const ConvGroupMember *m, const std::vector<int> &
 // Times every variant of one pass and length on the group's members (run flags ignored) and
 // returns the fastest.
 template <typename T>
-mm_status group_tune(const GDesc<T> *d, const ConvGroupMember *m, const std::vector<int> &mem, int pass, int len,
+mm_status group_tune(const ConvGroup *g, const ConvGroupMember *m, const std::vector<int> &mem, int pass, int len,
                      cudaStream_t st, int *best)
 {
 	*best = 0;
@@ -1820,6 +1975,8 @@ mm_status group_tune(const GDesc<T> *d, const ConvGroupMember *m, const std::vec
 	mm_status r = MM_OK;
 	for (int v = 0; v < GRP_VARIANTS && r == MM_OK; ++v) {
 		if (!group_threads<T>(pass, len, v) || group_smem_bytes<T>(pass, len, v) > 227 * 1024) continue;
+		if (v == 3 && !g->maps_ok) continue;
+		const int grid = v == 3 ? group_grid<T>(pass, len) : 0;
 		const std::vector<int2> items = group_items<T>(m, mem, pass, len, v);
 		int2 *di = nullptr;
 		r = cuda_status(cudaMalloc(&di, sizeof(int2) * items.size()), "cudaMalloc");
@@ -1827,9 +1984,9 @@ mm_status group_tune(const GDesc<T> *d, const ConvGroupMember *m, const std::vec
 		                                                cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
 		if (r == MM_OK) r = group_smem<T>(pass, len, v);
 		if (r == MM_OK) {
-			group_launch_v<T>(d, pass, len, v, di, (int)items.size(), 0, 0, st);  // warm-up
+			group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, st);  // warm-up
 			cudaEventRecord(e0, st);
-			for (int k = 0; k < 3; ++k) group_launch_v<T>(d, pass, len, v, di, (int)items.size(), 0, 0, st);
+			for (int k = 0; k < 3; ++k) group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, st);
 			cudaEventRecord(e1, st);
 			r = cuda_status(cudaEventSynchronize(e1), "autotune launch");
 		}
@@ -1875,6 +2032,32 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 	}
 	MM_CUDA(cudaMalloc(&g->desc, sizeof(GDesc<T>) * count));
 	MM_CUDA(cudaMemcpyAsync(g->desc, h.data(), sizeof(GDesc<T>) * count, cudaMemcpyHostToDevice, st));
+	// tensor maps of the TMA-staged y passes (variant 3): every member's spectrum, forward view of
+	// its ny data rows (zero fill to N/2), inverse view of all py rows
+	{
+		std::vector<CUtensorMap> maps(2 * (size_t)count);
+		bool ok = true;
+		for (int i = 0; i < count && ok; ++i) {
+			const ConvPlan *p = m[i].plan;
+			const int E = (int)(sizeof(cplx<T>) / 8), tb = ct_tb(p->py, (int)sizeof(cplx<T>));
+			if (2 * p->ny > p->py || tb * (int)sizeof(cplx<T>) < 16 || tb * E > 256) { ok = false; break; }
+			const int rows_f = p->py / 2, rows_i = p->py;
+			const uint64_t d0 = (uint64_t)p->lx * E, rowb = (uint64_t)p->lx * sizeof(cplx<T>), planeb = rowb * p->py;
+			ok = tma_encode_3d(&maps[2 * i], p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, tb * E,
+			                   rows_f < 256 ? rows_f : 256, 1) == MM_OK &&
+			     tma_encode_3d(&maps[2 * i + 1], p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, tb * E,
+			                   rows_i < 256 ? rows_i : 256, 1) == MM_OK;
+		}
+		if (ok) {
+			MM_CUDA(cudaMalloc(&g->maps, sizeof(CUtensorMap) * maps.size()));
+			MM_CUDA(cudaMemcpyAsync(g->maps, maps.data(), sizeof(CUtensorMap) * maps.size(), cudaMemcpyHostToDevice, st));
+			MM_CUDA(cudaMalloc(&g->err, sizeof(int)));
+			MM_CUDA(cudaMemsetAsync(g->err, 0, sizeof(int), st));
+			g->maps_ok = true;
+		} else {
+			clear_error();
+		}
+	}
 	for (const auto &kv : lists) {
 		const int pass = kv.first.first, len = kv.first.second;
 		int v = 0;
@@ -1891,12 +2074,13 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 			known = true;
 		}
 		if (!known) {
-			MM_TRY(group_tune<T>((const GDesc<T> *)g->desc, m, kv.second, pass, len, st, &v));
+			MM_TRY(group_tune<T>(g, m, kv.second, pass, len, st, &v));
 			std::lock_guard<std::mutex> lock(g_tune_mu);
 			g_tuned[std::make_tuple(g->prec, pass, len)] = v;
 		}
 		const std::vector<int2> items = group_items<T>(m, kv.second, pass, len, v);
-		ConvGroup::List l{pass, len, v, nullptr, (int)items.size()};
+		if (v == 3 && !g->maps_ok) v = 0;
+		ConvGroup::List l{pass, len, v, nullptr, (int)items.size(), v == 3 ? group_grid<T>(pass, len) : 0};
 		MM_CUDA(cudaMalloc(&l.items, sizeof(int2) * l.n));
 		MM_CUDA(cudaMemcpyAsync(l.items, items.data(), sizeof(int2) * l.n, cudaMemcpyHostToDevice, st));
 		MM_TRY(group_smem<T>(pass, len, v));

@@ -50,6 +50,7 @@ class ServeStats:
     rebuilds: int = 0
     rounds: int = 0
     peak_resident: int = 0
+    unfinished: int = 0  # requests not finished when the deadline passed
 
     def percentile(self, q: float) -> float:
         return float(np.percentile([c.latency for c in self.completed], q)) if self.completed else float("nan")
@@ -70,7 +71,9 @@ class Server:
         self.rounds_per_tick = int(rounds_per_tick)
         self.keep_results = keep_results
 
-    def run(self, requests: List[Request], clock=time.perf_counter) -> ServeStats:
+    def run(self, requests: List[Request], clock=time.perf_counter, deadline: Optional[float] = None) -> ServeStats:
+        """Serves `requests`; with `deadline` (seconds) it stops admitting and running once the
+        deadline has passed and counts the requests left over in `unfinished`."""
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         live = {}  # slot -> (request, resident bytes, admitted)
         used = 0
@@ -78,6 +81,8 @@ class Server:
         t0 = clock()
         while pending or live:
             now = clock() - t0
+            if deadline is not None and now > deadline:
+                break
             while pending and pending[0].arrival <= now:
                 req = pending[0]
                 res, trans = req.instance.device_bytes(self.precision)
@@ -109,6 +114,9 @@ class Server:
                     used -= res
                     stats.rebuilds += 1
         stats.makespan = clock() - t0
+        stats.unfinished = len(pending) + len(live)
+        for slot in list(live):
+            self.batch.remove(slot)
         return stats
 
     def close(self) -> None:

@@ -98,7 +98,7 @@ def test_batch_instances_follow_the_single_solver(bt, sv, monkeypatch):
     # the autotuner's other variants factor the FFTs differently: rounding-level differences,
     # checked in FP64 (in FP32 such differences move the adaptive step sizes, so FP32 runs are
     # compared at equal times, not at equal step counts)
-    for variant in (1, 2):
+    for variant in (1, 2, 3):
         for (r, st, got, ref), q in zip(run_pair(bt, sv, insts, "f64", variant, monkeypatch), insts):
             assert st["steps"] == r["steps"] and st["t"] == pytest.approx(r["t"], rel=1e-8)
             assert float((got - ref).abs().max()) / q.Ms < 1e-8

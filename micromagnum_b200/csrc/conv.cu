@@ -1733,6 +1733,126 @@ __global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)),
 	}
 }
 
+// Fused y and z passes for small members (the autotuner-free path of the grouped convolution):
+// one CTA takes a tile of TB x-frequency columns of one member and keeps all of its y-z data in
+// shared memory: the forward y transforms of the 3*NZ (component, z) lines of every column (ny
+// data rows, zero padded to PY), the z transform, tensor multiply and inverse z transform of every
+// (ky, column) in registers (3 components x PZ values per thread, the zero half of each z column
+// skipped), and the inverse y transforms, whose rows y < ny go back to HBM.  The full y spectrum
+// never reaches HBM: the pass reads and writes the x-transformed rows once and reads the tensor.
+// Lines are split into G groups of LG lines so that a group's transform needs at most 512 threads
+// (128 registers per thread for the z columns).
+template <int PY, int PZ, class C>
+struct YZGeom {
+	static constexpr int NZ = PZ / 2;  // planes a member of this group can have (nz <= pz/2)
+	static constexpr int R = ct_radix(PY), TPL = PY / R;
+	static constexpr size_t line_bytes = (size_t)PY * sizeof(C);
+	static constexpr int tb_for(int tb)
+	{
+		return (tb > 1 && (size_t)3 * NZ * tb * line_bytes * 33 / 32 > 200 * 1024) ? tb_for(tb / 2) : tb;
+	}
+	static constexpr int TB = tb_for(8);
+	static constexpr int L = 3 * NZ * TB;
+	static constexpr int g_for(int g) { return ((L / g) * TPL > 512 && L % (2 * g) == 0) ? g_for(g * 2) : g; }
+	static constexpr int G = g_for(1);
+	static constexpr int LG = L / G;
+	static constexpr int THREADS = LG * TPL;
+	static constexpr size_t GROUP_ELEMS = SmCols<PY, LG>::SIZE;
+	static constexpr size_t SMEM = (size_t)G * GROUP_ELEMS * sizeof(C);
+	static constexpr bool fits = SMEM <= 227 * 1024 && THREADS >= 32 && THREADS <= 1024 && L % G == 0;
+};
+
+template <typename T, int PY, int PZ>
+__global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
+    k_yz_grp(const GDesc<T> *__restrict__ d, const int2 *__restrict__ items, int gate)
+{
+	using C = cplx<T>;
+	using G = YZGeom<PY, PZ, C>;
+	constexpr int TB = G::TB, LG = G::LG, NZ = G::NZ, H = PZ / 2;
+	using SI = SmCols<PY, LG>;
+	const int2 it = items[blockIdx.x];
+	if (member_skips(d[it.x].flags, gate)) return;
+	const GDesc<T> &g = d[it.x];
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	C *smem = reinterpret_cast<C *>(smem_raw);
+	const int tid = threadIdx.x;
+	const int nz = g.nz, ny = g.ny, hx = g.hx, lx = g.lx;
+	const int kx0 = it.y * TB;
+	// line l = (c * NZ + z) * TB + col of group l / LG
+	auto elem = [&](int l, int k) -> C & { return smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, k)]; };
+	// forward y transforms
+	for (int grp = 0; grp < G::G; ++grp) {
+		const int line = tid % LG, j0 = tid / LG;
+		const int l = grp * LG + line;
+		const int col = l % TB, cz = l / TB, c = cz / NZ, z = cz % NZ;
+		const int kx = kx0 + col;
+		const bool ok = kx < hx && z < nz;
+		const C *src = g.spec + ((size_t)(c * nz + (ok ? z : 0)) * g.py) * lx + (ok ? kx : 0);
+		auto ld = [&](int, int y) -> C { return (ok && y < ny) ? src[(size_t)y * lx] : C{0, 0}; };
+		C *sm = smem + (size_t)grp * G::GROUP_ELEMS;
+		auto st = [&](int ll, int k, C v) { sm[SI::at(ll, k)] = v; };
+		cta_fft<T, PY, G::R, LG, false, SI>(sm, g.tw_y, line, j0, ld, st);
+	}
+	__syncthreads();
+	// z transforms, tensor multiply, inverse z transforms: one thread per (ky, column)
+	const size_t cs = (size_t)g.qz * g.qy * hx, kzs = (size_t)g.qy * hx;
+	for (int item = tid; item < PY * TB; item += G::THREADS) {
+		const int col = item % TB, ky = item / TB;
+		const int kx = kx0 + col;
+		if (kx >= hx) continue;
+		C v[3][PZ];
+#pragma unroll
+		for (int c = 0; c < 3; ++c) {
+#pragma unroll
+			for (int z = 0; z < H; ++z) v[c][z] = z < nz ? elem((c * NZ + (z < NZ ? z : 0)) * TB + col, ky) : C{0, 0};
+			dft_reg_halfzero<T, PZ>(v[c]);
+		}
+		const bool fy = ky > PY / 2;
+		const int kyr = fy ? PY - ky : ky;
+		const T sy = fy ? T(-1) : T(1);
+#pragma unroll
+		for (int p = 0; p < PZ; ++p) {
+			const int kz = brev<PZ>(p);
+			const bool fz = kz > PZ / 2;
+			const int kzr = fz ? PZ - kz : kz;
+			const T sz = fz ? T(-1) : T(1);
+			const T *t = g.tensor + (size_t)kzr * kzs + (size_t)kyr * hx + kx;
+			C m0 = v[0][p], m1 = v[1][p], m2 = v[2][p];
+			tensor_apply<T, C>(t, cs, sy, sz, m0, m1, m2);
+			v[0][p] = m0;
+			v[1][p] = m1;
+			v[2][p] = m2;
+		}
+#pragma unroll
+		for (int c = 0; c < 3; ++c) {
+			C w[PZ];
+#pragma unroll
+			for (int k = 0; k < PZ; ++k) w[k] = v[c][brev<PZ>(k)];  // natural order for the inverse
+			dft_reg<T, PZ, true>(w);
+#pragma unroll
+			for (int z = 0; z < H; ++z)
+				if (z < nz && z < NZ) elem((c * NZ + z) * TB + col, ky) = w[brev<PZ>(z)];
+		}
+	}
+	__syncthreads();
+	// inverse y transforms, rows y < ny to HBM
+	for (int grp = 0; grp < G::G; ++grp) {
+		const int line = tid % LG, j0 = tid / LG;
+		const int l = grp * LG + line;
+		const int col = l % TB, cz = l / TB, c = cz / NZ, z = cz % NZ;
+		const int kx = kx0 + col;
+		const bool ok = kx < hx && z < nz;
+		C *dst = g.spec + ((size_t)(c * nz + (ok ? z : 0)) * g.py) * lx + (ok ? kx : 0);
+		C *sm = smem + (size_t)grp * G::GROUP_ELEMS;
+		auto ld = [&](int ll, int k) -> C { return sm[SI::at(ll, k)]; };
+		auto st = [&](int, int y, C val) {
+			if (ok && y < ny) dst[(size_t)y * lx] = val;
+		};
+		if (grp > 0) __syncthreads();
+		cta_fft<T, PY, G::R, LG, true, SI, true>(sm, g.tw_y, line, j0, ld, st);
+	}
+}
+
 } // namespace
 
 struct ConvGroup {
@@ -1740,7 +1860,7 @@ struct ConvGroup {
 	int count = 0;
 	void *desc = nullptr;  // GDesc<T>[count]
 	struct List {
-		int pass;     // 0 x forward, 1 y forward, 2 z, 3 y inverse, 4 x inverse
+		int pass;     // 0 x forward, 1 y forward, 2 z, 3 y inverse, 4 x inverse, 6 fused y+z (len = py*64+pz)
 		int len;      // transform length of the pass
 		int variant;  // tile shape chosen by the autotuner (GRP_VARIANTS)
 		int2 *items;
@@ -1780,12 +1900,53 @@ void with_len_variant(int len, int v, F &&f)
 #undef MM_WLV
 }
 
+// Calls f(integral_constant PY, integral_constant PZ) for a fused y+z pass key (py * 64 + pz).
+template <class F>
+void with_yz(int key, F &&f)
+{
+	const int py = key / 64, pz = key % 64;
+	auto by_pz = [&](auto pyc) {
+		switch (pz) {
+		case 2: f(pyc, std::integral_constant<int, 2>()); break;
+		case 4: f(pyc, std::integral_constant<int, 4>()); break;
+		case 8: f(pyc, std::integral_constant<int, 8>()); break;
+		}
+	};
+	switch (py) {
+	case 16: by_pz(std::integral_constant<int, 16>()); break;
+	case 32: by_pz(std::integral_constant<int, 32>()); break;
+	case 64: by_pz(std::integral_constant<int, 64>()); break;
+	case 128: by_pz(std::integral_constant<int, 128>()); break;
+	case 256: by_pz(std::integral_constant<int, 256>()); break;
+	case 512: by_pz(std::integral_constant<int, 512>()); break;
+	}
+}
+
+// Whether a member takes the fused y+z pass (and its columns per CTA).
+template <typename T>
+int yz_tb(const ConvPlan *p)
+{
+	int tb = 0;
+	if (p->py < 16 || p->py > 512 || (p->pz != 2 && p->pz != 4 && p->pz != 8) || 2 * p->nz > p->pz) return 0;
+	with_yz(p->py * 64 + p->pz, [&](auto pyc, auto pzc) {
+		using G = YZGeom<decltype(pyc)::value, decltype(pzc)::value, cplx<T>>;
+		if constexpr (G::fits) tb = G::TB;
+	});
+	return tb;
+}
+
 // Threads of one CTA of a pass/length/variant (0 when the variant does not exist).
 template <typename T>
 int group_threads(int pass, int len, int v)
 {
 	using C = cplx<T>;
 	if (pass == 2) return v == 0 ? ZR_THREADS : 0;
+	if (pass == 6) {
+		int t = 0;
+		if (v == 0)
+			with_yz(len, [&](auto pyc, auto pzc) { t = YZGeom<decltype(pyc)::value, decltype(pzc)::value, C>::THREADS; });
+		return t;
+	}
 	if (v == 3) {
 		if (pass != 1 && pass != 3) return 0;
 		const int tb = ct_tb(len, (int)sizeof(C));
@@ -1809,6 +1970,10 @@ int group_blocks(const ConvPlan *p, int pass, int len, int v)
 		const int lpb = var_lpb(len, csz, v);
 		return ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
 	}
+	if (pass == 6) {
+		const int tb = yz_tb<T>(p);
+		return (p->hx + tb - 1) / tb;
+	}
 	if (pass == 1 || pass == 3) {
 		const int tb = var_tb(len, csz, v == 3 ? 0 : v);
 		return (p->hx + tb - 1) / tb * 3 * p->nz;
@@ -1822,6 +1987,10 @@ size_t group_smem_bytes(int pass, int len, int v)
 	using C = cplx<T>;
 	size_t r = 0;
 	if (pass == 2) return (size_t)2 * len * 96 * sizeof(C);
+	if (pass == 6) {
+		with_yz(len, [&](auto pyc, auto pzc) { r = YZGeom<decltype(pyc)::value, decltype(pzc)::value, C>::SMEM; });
+		return r;
+	}
 	if (v == 3) {
 		auto y3 = [&](auto nc) {
 			constexpr int N = decltype(nc)::value, TB = ct_tb(N, sizeof(C));
@@ -1846,6 +2015,13 @@ mm_status group_smem(int pass, int len, int v)
 	using C = cplx<T>;
 	mm_status r = MM_OK;
 	const size_t sm = group_smem_bytes<T>(pass, len, v);
+	if (pass == 6) {
+		with_yz(len, [&](auto pyc, auto pzc) {
+			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
+			if constexpr (YZGeom<PY, PZ, C>::fits) r = set_smem<T>((const void *)k_yz_grp<T, PY, PZ>, sm);
+		});
+		return r;
+	}
 	if (pass == 2) {
 		switch (len) {
 		case 2: r = set_smem<T>((const void *)k_z_grp<T, 2>, sm); break;
@@ -1884,6 +2060,14 @@ void group_launch_v(const ConvGroup *g, int pass, int len, int v, const int2 *it
 	using C = cplx<T>;
 	const GDesc<T> *d = (const GDesc<T> *)g->desc;
 	const size_t sm = group_smem_bytes<T>(pass, len, v);
+	if (pass == 6) {
+		with_yz(len, [&](auto pyc, auto pzc) {
+			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
+			using G = YZGeom<PY, PZ, C>;
+			if constexpr (G::fits) k_yz_grp<T, PY, PZ><<<n, G::THREADS, sm, st>>>(d, items, gate);
+		});
+		return;
+	}
 	if (v == 3) {
 		auto y3 = [&](auto nc) {
 			constexpr int N = decltype(nc)::value, TB = ct_tb(N, sizeof(C));
@@ -2025,9 +2209,13 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
 		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
 		lists[{0, p->px}].push_back(i);
-		lists[{1, p->py}].push_back(i);
-		lists[{2, p->pz}].push_back(i);
-		lists[{3, p->py}].push_back(i);
+		if (yz_tb<T>(p) > 0) {
+			lists[{6, p->py * 64 + p->pz}].push_back(i);  // y, z and the multiply in one pass
+		} else {
+			lists[{1, p->py}].push_back(i);
+			lists[{2, p->pz}].push_back(i);
+			lists[{3, p->py}].push_back(i);
+		}
 		lists[{4, p->px}].push_back(i);
 	}
 	MM_CUDA(cudaMalloc(&g->desc, sizeof(GDesc<T>) * count));
@@ -2073,6 +2261,7 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 			v = (f >= 0 && f < GRP_VARIANTS && group_threads<T>(pass, len, f)) ? f : 0;
 			known = true;
 		}
+		if (pass == 6) known = true, v = 0;  // one variant
 		if (!known) {
 			MM_TRY(group_tune<T>(g, m, kv.second, pass, len, st, &v));
 			std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -2087,8 +2276,9 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		g->lists.push_back(l);
 	}
 	// lists in pass order (x forward, y forward, z, y inverse, x inverse)
+	auto rank = [](int pass) { return pass == 6 ? 1 : (pass >= 1 ? pass + 1 : pass); };
 	std::stable_sort(g->lists.begin(), g->lists.end(),
-	                 [](const ConvGroup::List &a, const ConvGroup::List &b) { return a.pass < b.pass; });
+	                 [&](const ConvGroup::List &a, const ConvGroup::List &b) { return rank(a.pass) < rank(b.pass); });
 	for (int i = 0; i < count; ++i) h[i].flags = m[i].flags;
 	MM_CUDA(cudaMemcpyAsync(g->desc, h.data(), sizeof(GDesc<T>) * count, cudaMemcpyHostToDevice, st));
 	MM_CUDA(cudaStreamSynchronize(st));

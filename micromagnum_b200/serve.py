@@ -1,18 +1,22 @@
 """Serving: a request loop with continuous batching over `Batch`.
 
-Requests (a relax or a timed switching solve of one box, with its arrival time) are admitted in
-arrival order as soon as they have arrived and their device memory fits the budget; admitted
-requests join the lock-step rounds of the running ones (their tensor and spectra are built while
-the others' rounds are on the device), keep their state, tensor and spectra resident until they
-finish, and leave the batch, freeing their memory, as soon as they finish.  Latency is the time
-from a request's arrival to the host seeing its result.
+Requests (a relax or a timed switching solve of one box, with its arrival time) go, by size, to
+one of a few size classes.  Each class is a `Batch` driven by its own host thread on its own CUDA
+stream, so the classes' rounds overlap on the device and a small request never waits for the
+rounds of a large one.  Within a class, requests are admitted in arrival order as soon as they
+have arrived and their device memory (resident + set-up peak) fits the shared budget; admitted
+requests join the running ones' lock-step rounds at the next tick (their tensor and spectra are
+built while the other rounds run), keep state, tensor and spectra resident until they finish,
+and leave the batch, freeing their memory, as soon as they finish.  Latency is the time from a
+request's arrival to the host seeing its result.
 """
 from __future__ import annotations
 
+import threading
 import time
 from collections import deque
 from dataclasses import dataclass, field
-from typing import List, Optional
+from typing import List, Optional, Sequence
 
 import numpy as np
 
@@ -60,64 +64,119 @@ class ServeStats:
         return len(self.completed) / self.makespan if self.makespan > 0 else 0.0
 
 
+class _Class:
+    """One size class: a batch, its queue of arrived requests and its running requests."""
+
+    def __init__(self, batch: Batch):
+        self.batch = batch
+        self.queue = deque()
+        self.live = {}  # slot -> (request, resident bytes, admitted)
+
+
 class Server:
     def __init__(self, memory_budget: int, precision: str = "f32", eps_abs: float = 1e-3, eps_rel: float = 1e-4,
                  max_torque: float = 1e-4, check_every_nth_step: int = 1, rounds_per_tick: int = 8,
-                 keep_results: bool = False):
+                 keep_results: bool = False, class_bounds: Sequence[int] = (1 << 17, 1 << 20)):
+        """class_bounds: upper cell counts of the size classes (a last class takes the rest)."""
         self.budget = int(memory_budget)
-        self.batch = Batch([], precision=precision, eps_abs=eps_abs, eps_rel=eps_rel, max_torque=max_torque,
-                           check_every_nth_step=check_every_nth_step)
         self.precision = precision
         self.rounds_per_tick = int(rounds_per_tick)
         self.keep_results = keep_results
+        self.bounds = list(class_bounds)
+        self.classes = [_Class(Batch([], precision=precision, eps_abs=eps_abs, eps_rel=eps_rel,
+                                     max_torque=max_torque, check_every_nth_step=check_every_nth_step))
+                        for _ in range(len(self.bounds) + 1)]
+
+    def _class_of(self, req: Request) -> _Class:
+        n = req.instance.n
+        for b, c in zip(self.bounds, self.classes):
+            if n <= b:
+                return c
+        return self.classes[-1]
 
     def run(self, requests: List[Request], clock=time.perf_counter, deadline: Optional[float] = None) -> ServeStats:
         """Serves `requests`; with `deadline` (seconds) it stops admitting and running once the
         deadline has passed and counts the requests left over in `unfinished`."""
-        pending = deque(sorted(requests, key=lambda r: r.arrival))
-        live = {}  # slot -> (request, resident bytes, admitted)
-        used = 0
         stats = ServeStats()
+        lock = threading.Lock()
+        state = {"used": 0, "dispatching": True}
         t0 = clock()
-        while pending or live:
-            now = clock() - t0
-            if deadline is not None and now > deadline:
+        for r in requests:
+            need = sum(r.instance.device_bytes(self.precision))
+            if need > self.budget:
+                raise MemoryError(f"request {r.id} needs {need} bytes, over the budget {self.budget}")
+
+        def expired():
+            return deadline is not None and clock() - t0 > deadline
+
+        def worker(cl: _Class):
+            while not expired():
+                admitted = False
+                while True:  # admit in arrival order while memory allows
+                    with lock:
+                        if not cl.queue:
+                            break
+                        req = cl.queue[0]
+                        res, trans = req.instance.device_bytes(self.precision)
+                        if cl.live and state["used"] + res + trans > self.budget:
+                            break
+                        state["used"] += res
+                        stats.peak_resident = max(stats.peak_resident, state["used"])
+                        cl.queue.popleft()
+                    slot = cl.batch.add(req.instance, req.M0)
+                    cl.live[slot] = (req, res, clock() - t0)
+                    admitted = True
+                if not cl.live:
+                    with lock:
+                        if not state["dispatching"] and not cl.queue:
+                            return
+                    time.sleep(0.0005)
+                    continue
+                rounds = cl.batch.relax(max_rounds=self.rounds_per_tick, check_interval=self.rounds_per_tick)
+                results = cl.batch.results()
+                now = clock() - t0
+                done = []
+                for slot in list(cl.live):
+                    r = results[slot]
+                    if r["status"] in (1, 2):
+                        req, res, adm = cl.live.pop(slot)
+                        M = cl.batch.get_M(slot).cpu().numpy() if self.keep_results else None
+                        done.append((Completed(req.id, r["status"], req.arrival, adm, now, r["steps"], r["attempts"],
+                                               M), slot, res))
+                for c, slot, res in done:
+                    cl.batch.remove(slot)
+                with lock:
+                    stats.rounds += rounds
+                    stats.rebuilds += len(done) + (1 if admitted else 0)
+                    for c, slot, res in done:
+                        stats.completed.append(c)
+                        state["used"] -= res
+
+        threads = [threading.Thread(target=worker, args=(cl,), daemon=True) for cl in self.classes]
+        for th in threads:
+            th.start()
+        for req in sorted(requests, key=lambda r: r.arrival):  # dispatch at arrival times
+            wait = req.arrival - (clock() - t0)
+            if wait > 0:
+                time.sleep(wait)
+            if expired():
                 break
-            while pending and pending[0].arrival <= now:
-                req = pending[0]
-                res, trans = req.instance.device_bytes(self.precision)
-                if live and used + res + trans > self.budget:
-                    break  # wait until running requests free memory
-                if res + trans > self.budget:
-                    raise MemoryError(f"request {req.id} needs {res + trans} bytes, over the budget {self.budget}")
-                slot = self.batch.add(req.instance, req.M0)
-                used += res
-                stats.peak_resident = max(stats.peak_resident, used)
-                live[slot] = (req, res, clock() - t0)
-                pending.popleft()
-                stats.rebuilds += 1
-            if not live:
-                if pending:
-                    time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
-                continue
-            stats.rounds += self.batch.relax(max_rounds=self.rounds_per_tick, check_interval=self.rounds_per_tick)
-            results = self.batch.results()
-            now = clock() - t0
-            for slot in list(live):
-                r = results[slot]
-                if r["status"] in (1, 2):
-                    req, res, adm = live.pop(slot)
-                    M = self.batch.get_M(slot).cpu().numpy() if self.keep_results else None
-                    stats.completed.append(Completed(req.id, r["status"], req.arrival, adm, now, r["steps"],
-                                                     r["attempts"], M))
-                    self.batch.remove(slot)
-                    used -= res
-                    stats.rebuilds += 1
+            with lock:
+                self._class_of(req).queue.append(req)
+        with lock:
+            state["dispatching"] = False
+        for th in threads:
+            th.join()
         stats.makespan = clock() - t0
-        stats.unfinished = len(pending) + len(live)
-        for slot in list(live):
-            self.batch.remove(slot)
+        for cl in self.classes:
+            for slot in list(cl.live):
+                cl.batch.remove(slot)
+            cl.live.clear()
+            cl.queue.clear()
+        stats.unfinished = len(requests) - len(stats.completed)
+        stats.completed.sort(key=lambda c: c.id)
         return stats
 
     def close(self) -> None:
-        self.batch.close()
+        for cl in self.classes:
+            cl.batch.close()

@@ -1733,6 +1733,18 @@ __global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)),
 	}
 }
 
+// Asynchronous copy of one complex value global -> shared (LDGSTS, 8 or 16 bytes).
+template <class C>
+__device__ __forceinline__ void cp_async_c(C *dst, const C *src)
+{
+	const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+	if constexpr (sizeof(C) == 8)
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+	else
+		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all_c() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Fused y and z passes for small members (the autotuner-free path of the grouped convolution):
 // one CTA takes a tile of TB x-frequency columns of one member and keeps all of its y-z data in
 // shared memory: the forward y transforms of the 3*NZ (component, z) lines of every column (ny
@@ -1780,18 +1792,25 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 	const int kx0 = it.y * TB;
 	// line l = (c * NZ + z) * TB + col of group l / LG
 	auto elem = [&](int l, int k) -> C & { return smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, k)]; };
-	// forward y transforms
+	// the tile's x-transformed rows (y < ny) land in the groups' buffers by asynchronous copies
+	// issued all at once; lines outside the member (z >= nz, kx >= hx) are never stored
+	for (int e = tid; e < 3 * NZ * TB * ny; e += G::THREADS) {
+		const int col = e % TB, rest = e / TB, y = rest % ny, cz = rest / ny, c = cz / NZ, z = cz % NZ;
+		const int kx = kx0 + col;
+		if (z >= nz || kx >= hx) continue;
+		const int l = cz * TB + col;
+		cp_async_c(&smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, y)],
+		           g.spec + ((size_t)(c * nz + z) * g.py + y) * lx + kx);
+	}
+	cp_async_wait_all_c();
+	__syncthreads();
+	// forward y transforms in place (rows ny.. are the zero padding)
 	for (int grp = 0; grp < G::G; ++grp) {
 		const int line = tid % LG, j0 = tid / LG;
-		const int l = grp * LG + line;
-		const int col = l % TB, cz = l / TB, c = cz / NZ, z = cz % NZ;
-		const int kx = kx0 + col;
-		const bool ok = kx < hx && z < nz;
-		const C *src = g.spec + ((size_t)(c * nz + (ok ? z : 0)) * g.py) * lx + (ok ? kx : 0);
-		auto ld = [&](int, int y) -> C { return (ok && y < ny) ? src[(size_t)y * lx] : C{0, 0}; };
 		C *sm = smem + (size_t)grp * G::GROUP_ELEMS;
+		auto ld = [&](int ll, int y) -> C { return y < ny ? sm[SI::at(ll, y)] : C{0, 0}; };
 		auto st = [&](int ll, int k, C v) { sm[SI::at(ll, k)] = v; };
-		cta_fft<T, PY, G::R, LG, false, SI>(sm, g.tw_y, line, j0, ld, st);
+		cta_fft<T, PY, G::R, LG, false, SI, true>(sm, g.tw_y, line, j0, ld, st);
 	}
 	__syncthreads();
 	// z transforms, tensor multiply, inverse z transforms: one thread per (ky, column)
@@ -1871,12 +1890,21 @@ struct ConvGroup {
 	CUtensorMap *maps = nullptr;  // [2 member + inverse]: spectrum views of the y passes
 	bool maps_ok = false;         // every member's maps exist (variant 3 possible)
 	int *err = nullptr;           // set when a staged pass gave up waiting
+	// the lists of one phase (independent members) run side by side on these streams
+	static constexpr int POOL = 8;
+	cudaStream_t pool[POOL] = {};
+	cudaEvent_t fork = nullptr, join[POOL] = {};
 	~ConvGroup()
 	{
 		cudaFree(desc);
 		cudaFree(maps);
 		cudaFree(err);
 		for (auto &l : lists) cudaFree(l.items);
+		for (auto &q : pool)
+			if (q) cudaStreamDestroy(q);
+		for (auto &e : join)
+			if (e) cudaEventDestroy(e);
+		if (fork) cudaEventDestroy(fork);
 	}
 };
 
@@ -2293,6 +2321,15 @@ mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int
 	ConvGroup *g = new ConvGroup();
 	g->prec = members[0].plan ? members[0].plan->prec : MM_F32;
 	g->count = count;
+	mm_status rs = cuda_status(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming), "cudaEventCreate");
+	for (int q = 0; q < ConvGroup::POOL && rs == MM_OK; ++q) {
+		rs = cuda_status(cudaStreamCreateWithFlags(&g->pool[q], cudaStreamNonBlocking), "cudaStreamCreate");
+		if (rs == MM_OK) rs = cuda_status(cudaEventCreateWithFlags(&g->join[q], cudaEventDisableTiming), "cudaEventCreate");
+	}
+	if (rs != MM_OK) {
+		delete g;
+		return rs;
+	}
 	const mm_status r = g->prec == MM_F64 ? group_create<double>(g, members, count, st)
 	                                       : group_create<float>(g, members, count, st);
 	if (r != MM_OK) {
@@ -2303,13 +2340,38 @@ mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int
 	return MM_OK;
 }
 
+// The lists of one phase (x forward; y forward and fused y+z; z; y inverse; x inverse) touch
+// disjoint members, so each phase forks onto the group's stream pool and joins back on `st`
+// (inside a stream capture this becomes parallel graph branches).
 mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st)
 {
 	if (!g || input < 0 || input > 2) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad input selector");
-	for (const auto &l : g->lists) {
-		if (g->prec == MM_F64) group_launch<double>(g, l, input, gate, st);
-		else group_launch<float>(g, l, input, gate, st);
-		MM_TRY(after_launch("k_conv_grp"));
+	auto rank = [](int pass) { return pass == 6 ? 1 : pass; };
+	size_t i = 0;
+	while (i < g->lists.size()) {
+		size_t j = i;
+		while (j < g->lists.size() && rank(g->lists[j].pass) == rank(g->lists[i].pass)) ++j;
+		const int n = (int)(j - i);
+		if (n == 1) {
+			if (g->prec == MM_F64) group_launch<double>(g, g->lists[i], input, gate, st);
+			else group_launch<float>(g, g->lists[i], input, gate, st);
+			MM_TRY(after_launch("k_conv_grp"));
+		} else {
+			MM_CUDA(cudaEventRecord(g->fork, st));
+			const int used = n < ConvGroup::POOL ? n : ConvGroup::POOL;
+			for (int q = 0; q < used; ++q) MM_CUDA(cudaStreamWaitEvent(g->pool[q], g->fork, 0));
+			for (size_t k = i; k < j; ++k) {
+				cudaStream_t sq = g->pool[(k - i) % ConvGroup::POOL];
+				if (g->prec == MM_F64) group_launch<double>(g, g->lists[k], input, gate, sq);
+				else group_launch<float>(g, g->lists[k], input, gate, sq);
+				MM_TRY(after_launch("k_conv_grp"));
+			}
+			for (int q = 0; q < used; ++q) {
+				MM_CUDA(cudaEventRecord(g->join[q], g->pool[q]));
+				MM_CUDA(cudaStreamWaitEvent(st, g->join[q], 0));
+			}
+		}
+		i = j;
 	}
 	return MM_OK;
 }

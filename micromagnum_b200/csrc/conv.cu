@@ -1753,7 +1753,8 @@ __device__ __forceinline__ void cp_async_wait_all_c() { asm volatile("cp.async.w
 // skipped), and the inverse y transforms, whose rows y < ny go back to HBM.  The full y spectrum
 // never reaches HBM: the pass reads and writes the x-transformed rows once and reads the tensor.
 // Lines are split into G groups of LG lines so that a group's transform needs at most 512 threads
-// (128 registers per thread for the z columns).
+// (128 registers per thread for the z columns); tiles stay within ~104 KB of shared memory so
+// that two CTAs share an SM.
 template <int PY, int PZ, class C>
 struct YZGeom {
 	static constexpr int NZ = PZ / 2;  // planes a member of this group can have (nz <= pz/2)
@@ -1761,7 +1762,7 @@ struct YZGeom {
 	static constexpr size_t line_bytes = (size_t)PY * sizeof(C);
 	static constexpr int tb_for(int tb)
 	{
-		return (tb > 1 && (size_t)3 * NZ * tb * line_bytes * 33 / 32 > 200 * 1024) ? tb_for(tb / 2) : tb;
+		return (tb > 1 && (size_t)3 * NZ * tb * line_bytes * 33 / 32 > 104 * 1024) ? tb_for(tb / 2) : tb;
 	}
 	static constexpr int TB = tb_for(8);
 	static constexpr int L = 3 * NZ * TB;
@@ -1829,18 +1830,22 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 		const bool fy = ky > PY / 2;
 		const int kyr = fy ? PY - ky : ky;
 		const T sy = fy ? T(-1) : T(1);
+		// kz and PZ - kz share the tensor entries (sign of the z-odd components flipped): each
+		// reduced entry is loaded once
 #pragma unroll
-		for (int p = 0; p < PZ; ++p) {
-			const int kz = brev<PZ>(p);
-			const bool fz = kz > PZ / 2;
-			const int kzr = fz ? PZ - kz : kz;
-			const T sz = fz ? T(-1) : T(1);
+		for (int kzr = 0; kzr <= H; ++kzr) {
 			const T *t = g.tensor + (size_t)kzr * kzs + (size_t)kyr * hx + kx;
-			C m0 = v[0][p], m1 = v[1][p], m2 = v[2][p];
-			tensor_apply<T, C>(t, cs, sy, sz, m0, m1, m2);
-			v[0][p] = m0;
-			v[1][p] = m1;
-			v[2][p] = m2;
+			const T nxx = t[0], nxy = t[cs], nxz = t[2 * cs], nyy = t[3 * cs], nyz = t[4 * cs], nzz = t[5 * cs];
+#pragma unroll
+			for (int q = 0; q < ((kzr == 0 || kzr == H) ? 1 : 2); ++q) {
+				const int p = brev<PZ>(q ? PZ - kzr : kzr);
+				const T sz = q ? T(-1) : T(1);
+				const T xy = sy * nxy, xz = sz * nxz, yz = sy * sz * nyz;
+				const C m0 = v[0][p], m1 = v[1][p], m2 = v[2][p];
+				v[0][p] = C{nxx * m0.x + xy * m1.x + xz * m2.x, nxx * m0.y + xy * m1.y + xz * m2.y};
+				v[1][p] = C{xy * m0.x + nyy * m1.x + yz * m2.x, xy * m0.y + nyy * m1.y + yz * m2.y};
+				v[2][p] = C{xz * m0.x + yz * m1.x + nzz * m2.x, xz * m0.y + yz * m1.y + nzz * m2.y};
+			}
 		}
 #pragma unroll
 		for (int c = 0; c < 3; ++c) {

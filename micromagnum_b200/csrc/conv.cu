@@ -1766,20 +1766,17 @@ struct YZGeom {
 	}
 	static constexpr int TB = tb_for(8);
 	static constexpr int L = 3 * NZ * TB;
-	// groups: each component's NZ * TB lines (a power of two, so the skewed layout stays free of
-	// bank conflicts), split further until a group needs at most 512 threads
-	static constexpr int k_for(int k) { return ((NZ * TB / k) * TPL > 512 && (NZ * TB) % (2 * k) == 0) ? k_for(2 * k) : k; }
-	static constexpr int G = 3 * k_for(1);
+	static constexpr int g_for(int g) { return ((L / g) * TPL > 512 && L % (2 * g) == 0) ? g_for(g * 2) : g; }
+	static constexpr int G = g_for(1);
 	static constexpr int LG = L / G;
 	static constexpr int THREADS = LG * TPL;
 	static constexpr size_t GROUP_ELEMS = SmCols<PY, LG>::SIZE;
 	static constexpr size_t SMEM = (size_t)G * GROUP_ELEMS * sizeof(C);
-	static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;
 	static constexpr bool fits = SMEM <= 227 * 1024 && THREADS >= 32 && THREADS <= 1024 && L % G == 0;
 };
 
 template <typename T, int PY, int PZ>
-__global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS, YZGeom<PY, PZ, cplx<T>>::MINB)
+__global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
     k_yz_grp(const GDesc<T> *__restrict__ d, const int2 *__restrict__ items, int gate)
 {
 	using C = cplx<T>;

@@ -107,12 +107,12 @@ class Batch:
         """M of instance `index`, (3, N) or (3N,) in A/m (normalised to Ms in the material)."""
         v = torch.as_tensor(M, dtype=torch.float64).reshape(-1).cuda().contiguous()
         check(lib().mm_batch_set_M(self._h, int(index), ctypes.c_void_p(v.data_ptr()), None))
-        torch.cuda.synchronize()
+        torch.cuda.current_stream().synchronize()
 
     def get_M(self, index: int) -> torch.Tensor:
         out = torch.empty(3 * self.instances[index].n, dtype=torch.float64, device="cuda")
         check(lib().mm_batch_get_M(self._h, int(index), ctypes.c_void_p(out.data_ptr()), None))
-        torch.cuda.synchronize()
+        torch.cuda.current_stream().synchronize()
         return out.view(3, -1)
 
     def relax(self, max_rounds: int = 1_000_000, check_interval: int = 16) -> int:

@@ -27,6 +27,12 @@ int num_sms()
 
 // One scratch slot per device, created on first use and kept until process exit.  It holds the
 // accumulators of reductions whose result is returned to the host (energies, maxima).
+std::mutex &capture_mutex()
+{
+	static std::mutex mu;
+	return mu;
+}
+
 mm_status scalar_scratch(ScalarScratch **out)
 {
 	static std::mutex mu;

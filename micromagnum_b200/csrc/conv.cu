@@ -591,6 +591,23 @@ __global__ void __launch_bounds__(3 * TB * (PZ / ct_radix8(PZ))) k_z_ct(cplx<T> 
 	}
 }
 
+// Asynchronous copy of one real value global -> shared (LDGSTS, 4 or 8 bytes).
+template <typename T>
+__device__ __forceinline__ void cp_async_t(T *dst, const T *src)
+{
+	const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+	if constexpr (sizeof(T) == 4)
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+	else
+		asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all_t() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Shared memory of the register z pass: the spectrum of two rows (2 PZ kz x 3 components x 32 kx)
+// and the block's tensor entries ((PZ/2 + 1) x 6 x 32).
+template <typename T>
+constexpr size_t zr_smem(int pz) { return (size_t)2 * pz * 96 * 2 * sizeof(T) + (size_t)(pz / 2 + 1) * 192 * sizeof(T); }
+
 // ---- z pass in registers ------------------------------------------------------------------------
 // One thread per (kx, component, ky) column holds the whole length-PZ column in registers: the
 // forward DFT (upper half zero padding, nz <= PZ/2), the tensor multiply through shared memory,
@@ -616,6 +633,14 @@ __device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__r
 	const bool ok = (r == 0 || two) && kx < hx;
 	const size_t zstride = (size_t)py * lx;
 	C *col = S + ((size_t)c * nz * py + (size_t)(r == 0 ? b : b1)) * lx + kx;
+	// the block's tensor entries (kz' <= pz/2, 6 components, 32 kx at ky' = b) come in by
+	// asynchronous copies while the columns are loaded and transformed
+	T *tens = reinterpret_cast<T *>(sm + 2 * PZ * 96);
+	const size_t cs = (size_t)qz * qy * hx, kzs = (size_t)qy * hx;
+	for (int e = threadIdx.x; e < (H + 1) * 6 * 32; e += ZR_THREADS) {
+		const int kzr = e / 192, comp = (e / 32) % 6, kxx = bx * 32 + (e & 31);
+		if (kxx < hx) cp_async_t(&tens[e], Nt + comp * cs + kzr * kzs + (size_t)b * hx + kxx);
+	}
 	C v[PZ];
 #pragma unroll
 	for (int z = 0; z < H; ++z) v[z] = (ok && z < nz) ? col[z * zstride] : C{0, 0};
@@ -623,13 +648,12 @@ __device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__r
 	C *mine = sm + (r * PZ * 3 + c) * 32 + lane;
 #pragma unroll
 	for (int k = 0; k < PZ; ++k) mine[brev<PZ>(k) * 96] = v[k];
+	cp_async_wait_all_t();
 	__syncthreads();
 	if (kx < hx) {
-		const size_t cs = (size_t)qz * qy * hx, kzs = (size_t)qy * hx;
-		const T *tb = Nt + (size_t)b * hx + kx;
 		for (int kzr = w; kzr <= H; kzr += ZR_THREADS / 32) {
-			const T *t = tb + kzr * kzs;
-			const T nxx = t[0], nxy = t[cs], nxz = t[2 * cs], nyy = t[3 * cs], nyz = t[4 * cs], nzz = t[5 * cs];
+			const T *t = tens + kzr * 192 + lane;
+			const T nxx = t[0], nxy = t[32], nxz = t[64], nyy = t[96], nyz = t[128], nzz = t[160];
 			const int nk = (kzr == 0 || kzr == H) ? 1 : 2;
 			for (int rr = 0; rr < (two ? 2 : 1); ++rr) {
 				for (int q = 0; q < nk; ++q) {
@@ -667,7 +691,7 @@ template <typename T, int PZ>
 void fs_z_reg(ConvPlan *p, cudaStream_t st)
 {
 	const dim3 grid((p->hx + 31) / 32, p->qy);
-	k_z_reg<T, PZ><<<grid, ZR_THREADS, (size_t)2 * PZ * 96 * sizeof(cplx<T>), st>>>(
+	k_z_reg<T, PZ><<<grid, ZR_THREADS, zr_smem<T>(PZ), st>>>(
 	    (cplx<T> *)p->spec, (const T *)p->tensor, p->nz, p->py, p->hx, p->lx, p->qy, p->qz);
 }
 
@@ -1199,7 +1223,7 @@ mm_status fs_setup(ConvPlan *p)
 #undef MM_YTSETUP
 	p->reg_z = p->fast_z && 2 * p->nz <= p->pz && p->pz <= (sizeof(T) == 4 ? 32 : 16);
 	if (p->reg_z) {
-		const size_t sz = (size_t)2 * p->pz * 96 * sizeof(cplx<T>);
+		const size_t sz = zr_smem<T>(p->pz);
 		switch (p->pz) {
 		case 2: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 2>, sz)); break;
 		case 4: MM_TRY(set_smem<T>((const void *)k_z_reg<T, 4>, sz)); break;
@@ -2019,7 +2043,7 @@ size_t group_smem_bytes(int pass, int len, int v)
 {
 	using C = cplx<T>;
 	size_t r = 0;
-	if (pass == 2) return (size_t)2 * len * 96 * sizeof(C);
+	if (pass == 2) return zr_smem<T>(len);
 	if (pass == 6) {
 		with_yz(len, [&](auto pyc, auto pzc) { r = YZGeom<decltype(pyc)::value, decltype(pzc)::value, C>::SMEM; });
 		return r;

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <string>
 #include <atomic>
+#include <mutex>
 
 #include "../../include/mmb200.h"
 
@@ -178,6 +179,11 @@ __device__ __forceinline__ void block_sum_to(double *out, double v)
 		if (lane == 0) atomicAdd(out, w);
 	}
 }
+
+// Serialises, across host threads, stream captures of the batch rounds against calls that can
+// synchronise the whole device or allocate (instance set-up and tear-down): a device-wide
+// synchronisation while another thread captures would invalidate that capture.
+std::mutex &capture_mutex();
 
 // A small pinned host scalar buffer + device scratch for reductions returned to the host.
 struct ScalarScratch {

@@ -2017,6 +2017,7 @@ MM_API mm_status mm_batch_create(mm_batch **out, const mm_batch_config *cfg, int
 
 MM_API mm_status mm_batch_destroy(mm_batch *b)
 {
+	std::lock_guard<std::mutex> lock(capture_mutex());
 	free_batch(b);
 	return MM_OK;
 }
@@ -2026,6 +2027,7 @@ MM_API mm_status mm_batch_add(mm_batch *b, const mm_batch_instance *instance, co
 {
 	if (!b || !instance || !slot_out) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_add: invalid argument");
 	cudaStream_t st = as_stream(stream);
+	std::lock_guard<std::mutex> lock(capture_mutex());
 	return b->prec == MM_F64 ? add_instance<double>(b, *instance, mask_host, slot_out, st)
 	                         : add_instance<float>(b, *instance, mask_host, slot_out, st);
 }
@@ -2035,6 +2037,7 @@ MM_API mm_status mm_batch_remove(mm_batch *b, int slot)
 	mm_batch::Slot *sl = slot_of(b, slot);
 	if (!sl) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_remove: no such slot");
 	MM_CUDA(cudaStreamSynchronize(b->gs));
+	std::lock_guard<std::mutex> lock(capture_mutex());
 	free_solver(sl->s);
 	cudaFree(sl->dev);
 	*sl = mm_batch::Slot{};
@@ -2080,7 +2083,10 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 {
 	if (!b || max_rounds < 0 || check_interval < 1) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_relax: invalid argument");
 	cudaStream_t st = as_stream(stream);
-	if (b->dirty) MM_TRY(b->prec == MM_F64 ? build_rounds<double>(b, st) : build_rounds<float>(b, st));
+	if (b->dirty) {
+		std::lock_guard<std::mutex> lock(capture_mutex());
+		MM_TRY(b->prec == MM_F64 ? build_rounds<double>(b, st) : build_rounds<float>(b, st));
+	}
 	long long done = 0;
 	if (!b->members.empty()) {
 		const size_t cnt = b->members.size();

@@ -713,8 +713,17 @@ struct YTmaGeom {
 	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
 };
 
+// Columns per CTA of the single-instance TMA y pass: 32-byte rows, at most 256 threads, so that
+// two CTAs (and their barriers) interleave on an SM.
+__host__ __device__ constexpr int y_tma_tb(int n, int csize)
+{
+	int tb = ct_tb(n, csize);
+	while (tb * csize > 32 && tb * (n / ct_radix(n)) > 256) tb >>= 1;
+	return tb;
+}
+
 template <typename T, int N, int TB, bool INV>
-__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 1)
+__global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
     k_y_tma(const __grid_constant__ CUtensorMap tmap, cplx<T> *__restrict__ S, int n_out, int hx, int lx,
             int tiles_x, int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
@@ -977,7 +986,7 @@ template <typename T, int N>
 mm_status fs_setup_y_tma(ConvPlan *p)
 {
 	using C = cplx<T>;
-	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	constexpr int TB = y_tma_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
 	using GF = YTmaGeom<N, TB, false, C>;
 	using GI = YTmaGeom<N, TB, true, C>;
 	p->tma_y = false;
@@ -1006,7 +1015,7 @@ template <typename T, int N, bool INV>
 void fs_y_tma(ConvPlan *p, cudaStream_t st)
 {
 	using C = cplx<T>;
-	constexpr int TB = ct_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
+	constexpr int TB = y_tma_tb(N, sizeof(C)), THREADS = TB * (N / ct_radix(N));
 	using G = YTmaGeom<N, TB, INV, C>;
 	const int tiles_x = (p->hx + TB - 1) / TB, ntiles = tiles_x * 3 * p->nz;
 	const int grid = std::min(ntiles, INV ? p->grid_yi : p->grid_yf);

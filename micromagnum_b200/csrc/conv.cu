@@ -1491,6 +1491,12 @@ size_t ConvPlan::spec_bytes() const
 mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
                      const uint32_t *box)
 {
+	return tma_encode_as(map, base, rank, dims, strides, box, 8);
+}
+
+mm_status tma_encode_as(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
+                        const uint32_t *box, int esize)
+{
 	using Encode = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
 	                            const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
 	                            CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -1505,7 +1511,8 @@ mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_
 		}
 		encode = reinterpret_cast<Encode>(fn);
 	}
-	if (rank < 1 || rank > 5 || (reinterpret_cast<uintptr_t>(base) & 15) || ((box[0] * 8) & 15))
+	if (esize != 1 && esize != 4 && esize != 8) return fail(MM_ERR_INVALID_ARGUMENT, "tensor map element size");
+	if (rank < 1 || rank > 5 || (reinterpret_cast<uintptr_t>(base) & 15) || ((box[0] * esize) & 15))
 		return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map not 16-byte aligned");
 	cuuint64_t d[5], sb[4];
 	cuuint32_t bx[5], estr[5];
@@ -1519,7 +1526,10 @@ mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_
 		sb[i] = strides[i];
 		if (strides[i] & 15) return fail(MM_ERR_INVALID_ARGUMENT, "conv: tensor map stride not 16-byte aligned");
 	}
-	const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, (cuuint32_t)rank, const_cast<void *>(base), d, sb,
+	const CUtensorMapDataType dt = esize == 1   ? CU_TENSOR_MAP_DATA_TYPE_UINT8
+	                               : esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT32
+	                                            : CU_TENSOR_MAP_DATA_TYPE_UINT64;
+	const CUresult r = encode(map, dt, (cuuint32_t)rank, const_cast<void *>(base), d, sb,
 	                          bx, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
 	                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 	if (r != CUDA_SUCCESS)

@@ -25,8 +25,10 @@
 // rounding of the per-step increment; the controller runs in double.
 #include "mm_common.cuh"
 #include "conv.cuh"
+#include "tma.cuh"
 
 #include <vector>
+#include <cstdlib>
 #include <cstring>
 #include <cmath>
 #include <utility>
@@ -53,7 +55,8 @@ struct DevState {
 	double h_new;     // controller output
 	int accept;
 	int not_finite;
-	int pad[2];
+	int stage_timeout;  // set by a staged stage kernel whose bounded wait gave up
+	int pad;
 	double max_tq2;   // max (|m x H_eff| / Ms)^2 at the last stage's input (batched relaxations)
 };
 
@@ -161,46 +164,26 @@ __device__ __forceinline__ const DevMat<T> &mat_of(const CellArgs<T> &a, size_t 
 	return a.mat[a.reg ? a.reg[i] : 0];
 }
 
-// Effective field (without the demag term) and dm/dt of one cell of the unit-m field y.
-// Hd: demag field of the cell (added when the term is on); msr: Ms per region (shared memory).
-// The six neighbours are loaded once and serve both the exchange stencil and the Zhang-Li
-// gradient.  Returns false for empty cells.
+// Applied field at time t (constant part plus the linearly rising pulse).
 template <typename T>
-__device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restrict__ msr,
-                                         const T *__restrict__ y, size_t n, int x, int yy, int z, size_t i,
-                                         V3<T> Hd, double t, V3<T> &Heff, V3<T> &dm)
+__device__ __forceinline__ V3<T> zeeman_field(const CellArgs<T> &a, double t)
 {
-	const DevMat<T> &M = mat_of(a, i);
 	double f = 1.0;
 	if ((a.terms & MM_TERM_ZEEMAN) && a.rise > 0) f = t / a.rise < 1.0 ? t / a.rise : 1.0;
-	const V3<T> Hz = (a.terms & MM_TERM_ZEEMAN)
-	                     ? v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
-	                             (T)(a.Hext[2] + a.Hpulse[2] * f))
-	                     : v3<T>(0, 0, 0);
+	return (a.terms & MM_TERM_ZEEMAN) ? v3<T>((T)(a.Hext[0] + a.Hpulse[0] * f), (T)(a.Hext[1] + a.Hpulse[1] * f),
+	                                          (T)(a.Hext[2] + a.Hpulse[2] * f))
+	                                  : v3<T>(0, 0, 0);
+}
+
+// Field terms and dm/dt of one non-empty cell (material M, unit state m) from its gathered
+// neighbourhood: nb[q] / nms[q] are the unit state and Ms of the neighbours x-1, x+1, y-1, y+1,
+// z-1, z+1 (zero where the neighbour is outside the box).  Hd: demag field, Hz: applied field.
+template <typename T>
+__device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> &M, const V3<T> &m,
+                                          const V3<T> (&nb)[6], const T (&nms)[6], int x, int yy, int z,
+                                          V3<T> Hd, V3<T> Hz, V3<T> &Heff, V3<T> &dm)
+{
 	const T ms = M.Ms;
-	if (ms == T(0)) {
-		// empty cell: no magnetisation and no torque, but the stray and applied fields exist
-		// there (H_tot is the sum of the terms, each zero except these two)
-		Heff = ((a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0)) + Hz;
-		dm = v3<T>(0, 0, 0);
-		return false;
-	}
-	const V3<T> m = load3(y, i, n);
-	const size_t nxy = (size_t)a.nx * a.ny;
-	const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
-	const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
-	V3<T> nb[6];
-	T nms[6];
-#pragma unroll
-	for (int q = 0; q < 6; ++q) {
-		if (has[q]) {
-			nb[q] = load3(y, off[q], n);
-			nms[q] = a.reg ? msr[a.reg[off[q]]] : ms;
-		} else {
-			nb[q] = v3<T>(0, 0, 0);
-			nms[q] = T(0);
-		}
-	}
 	V3<T> H = (a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0);
 	if (a.terms & MM_TERM_EXCHANGE) {
 		// exchange_cpu.cpp:60-139: H = 2A/(mu0 Ms) sum_nb w (m_nb - m), empty neighbours skipped
@@ -250,6 +233,44 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 		const V3<T> mxu = cross(m, u);
 		dm = dm + M.zl1 * cross(m, mxu) + M.zl2 * mxu;
 	}
+}
+
+// Effective field (without the demag term) and dm/dt of one cell of the unit-m field y.
+// Hd: demag field of the cell (added when the term is on); msr: Ms per region (shared memory).
+// The six neighbours are loaded once and serve both the exchange stencil and the Zhang-Li
+// gradient.  Returns false for empty cells.
+template <typename T>
+__device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restrict__ msr,
+                                         const T *__restrict__ y, size_t n, int x, int yy, int z, size_t i,
+                                         V3<T> Hd, double t, V3<T> &Heff, V3<T> &dm)
+{
+	const DevMat<T> &M = mat_of(a, i);
+	const V3<T> Hz = zeeman_field(a, t);
+	const T ms = M.Ms;
+	if (ms == T(0)) {
+		// empty cell: no magnetisation and no torque, but the stray and applied fields exist
+		// there (H_tot is the sum of the terms, each zero except these two)
+		Heff = ((a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0)) + Hz;
+		dm = v3<T>(0, 0, 0);
+		return false;
+	}
+	const V3<T> m = load3(y, i, n);
+	const size_t nxy = (size_t)a.nx * a.ny;
+	const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
+	const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
+	V3<T> nb[6];
+	T nms[6];
+#pragma unroll
+	for (int q = 0; q < 6; ++q) {
+		if (has[q]) {
+			nb[q] = load3(y, off[q], n);
+			nms[q] = a.reg ? msr[a.reg[off[q]]] : ms;
+		} else {
+			nb[q] = v3<T>(0, 0, 0);
+			nms[q] = T(0);
+		}
+	}
+	cell_core<T>(a, M, m, nb, nms, x, yy, z, Hd, Hz, Heff, dm);
 	return true;
 }
 
@@ -273,6 +294,29 @@ struct StageCoef {
 	double bn[MAXS];  // b[i+1][0..i] (not last)  or  c[0..s-1] (last)
 	double ec[MAXS];  // error weights (last)
 };
+
+// Whether the combination of stage S reads k_l (uniform over a launch).
+__host__ __device__ inline bool stage_needs_k(const StageCoef &sc, int S, int l)
+{
+	return l < S && (sc.last ? (sc.ec[l] != 0.0 || (sc.write_new && sc.bn[l] != 0.0))
+	                         : ((sc.write_next && sc.bn[l] != 0.0) || (sc.reduce_k0 && l == 0)));
+}
+
+// Operand list of a staged stage launch, in order: the demag field (term on), y_n and its
+// compensation (when the stage writes a state), the k_l the combination reads.  Sets the operand
+// index of each (-1: not read) and returns the count.
+__host__ __device__ inline int stage_ops(const StageCoef &sc, int S, bool comp, bool demag, int *kop, int &op_hd,
+                                         int &op_hi, int &op_lo)
+{
+	int n = 0;
+	const bool out = sc.last ? sc.write_new : sc.write_next;
+	op_hd = demag ? n++ : -1;
+	op_hi = out ? n++ : -1;
+	op_lo = out && comp ? n++ : -1;
+#pragma unroll
+	for (int l = 0; l < MAXS; ++l) kop[l] = stage_needs_k(sc, S, l) ? n++ : -1;
+	return n;
+}
 
 // One fused stage: k_i = f(y_in) (demag field from Hd), then the next stage state
 // y_{i+1} = y_n + h sum_{l<=i} b_{i+1,l} k_l, or on the last stage the error maximum and y_{n+1}.
@@ -333,9 +377,7 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 	const bool out = sc.last ? sc.write_new : sc.write_next;
 	bool needk[MAXS];
 #pragma unroll
-	for (int l = 0; l < MAXS; ++l)
-		needk[l] = l < S && (sc.last ? (sc.ec[l] != 0.0 || (sc.write_new && sc.bn[l] != 0.0))
-		                             : ((sc.write_next && sc.bn[l] != 0.0) || (sc.reduce_k0 && l == 0)));
+	for (int l = 0; l < MAXS; ++l) needk[l] = stage_needs_k(sc, S, l);
 #pragma unroll
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
@@ -440,6 +482,325 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 	if (sc.reduce_k0) block_max_to(red_k0, k02);
 }
 
+// ---- Staged fused stage (single instance) -------------------------------------------------------
+// Column tiles of ST_X x ST_Y cells march through z.  A step (one tile plane) needs the stage input
+// y_in of planes z-1, z, z+1 with a one-cell halo in x and y, their region ids, and the per-cell
+// operands of plane z (stage_ops).  Everything arrives in shared memory by tensor-map copies
+// (cp.async.bulk.tensor) issued ST_AHEAD steps ahead by one thread: a halo plane is one box of
+// (ST_X + 8) x (ST_Y + 2) x 3 components starting at x0 - 4 (16-byte aligned; the box edges past
+// the grid read as zero and are never used, the stencil treats those neighbours as absent), its
+// region ids one box starting at x0 - 16, each operand one box of ST_X x ST_Y x 3.  Halo planes go
+// to a ring (each plane of a tile is loaded once), operands to ST_NOB buffers.  Each CTA
+// takes an equal contiguous range of the (tile, z) steps, so the work is balanced to one step.
+constexpr int ST_X = 64, ST_Y = 4;
+constexpr int ST_CPT = 1;                        // cells per consumer thread and step
+constexpr int ST_CONS = ST_X * ST_Y / ST_CPT;    // consumer threads (plus one producer warp)
+constexpr int ST_XH = ST_X + 8;   // y_in row: x0 - 4 .. x0 + ST_X + 4
+constexpr int ST_XR = ST_X + 32;  // region row: x0 - 16 .. x0 + ST_X + 16
+constexpr int ST_YH = ST_Y + 2;
+constexpr int ST_AHEAD = 1;             // steps whose copies are in flight while one is computed
+constexpr int ST_RING = ST_AHEAD + 3;   // halo planes: the three being read plus the ones arriving
+constexpr int ST_NOB = ST_AHEAD + 1;    // operand buffers
+
+// Tensor maps of one stage launch: the stage input, region ids, demag field, y_n and its
+// compensation, and every physical stage-vector buffer (the launch finds the buffer behind each
+// k_l of the device-side table, which first-same-as-last tableaus permute).
+struct StageMaps {
+	CUtensorMap yin, reg, hd, hi, lo;
+	CUtensorMap k[MAXS];
+	const void *kptr[MAXS];
+};
+
+template <typename T>
+struct StTmaGeom {
+	static constexpr size_t YSLOT = ((size_t)3 * ST_YH * ST_XH * sizeof(T) + 127) / 128 * 128;  // bytes
+	static constexpr size_t YBOX = (size_t)3 * ST_YH * ST_XH * sizeof(T);
+	static constexpr size_t RSLOT = ((size_t)ST_YH * ST_XR + 127) / 128 * 128;
+	static constexpr size_t RBOX = (size_t)ST_YH * ST_XR;
+	static constexpr size_t YB = ST_RING * YSLOT;
+	static constexpr size_t RB = ST_RING * RSLOT;
+	static constexpr size_t OPB = (size_t)3 * ST_Y * ST_X * sizeof(T);  // one operand, one plane
+	static constexpr size_t smem(int nops)
+	{
+		return YB + RB + ST_NOB * (size_t)nops * OPB + 8 * (ST_RING + 2 * ST_NOB);
+	}
+	static constexpr int MINB = sizeof(T) == 4 ? 3 : 1;
+};
+
+// Whether a box takes the staged stage kernel: rows of y_in (and of the region ids) start on
+// 16-byte boundaries.
+inline bool stage_tma_fits(int nx, size_t esize, bool regions)
+{
+	return (nx * esize) % 16 == 0 && (!regions || nx % 16 == 0);
+}
+
+template <typename T, bool COMP, int S>
+__global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
+    k_stage_tma(const __grid_constant__ StageMaps maps, CellArgs<T> a, StageCoef sc, const KTab<T> *__restrict__ ktab,
+                T *__restrict__ y_out, T *__restrict__ y_out_lo, DevState *__restrict__ st, int tiles_x,
+                int tiles_y)
+{
+	using G = StTmaGeom<T>;
+	__shared__ T msr[256];
+	__shared__ const CUtensorMap *opmap[MAXS + 3];
+	__shared__ T fb[MAXS], fe[MAXS];  // h b_l and h e_l at working precision
+	__shared__ int abort_flag;
+	extern __shared__ __align__(128) unsigned char smem_st[];
+	unsigned char *ys = smem_st;
+	uint8_t *rs = smem_st + G::YB;
+	T *os = reinterpret_cast<T *>(smem_st + G::YB + G::RB);
+	const bool demag = a.terms & MM_TERM_DEMAG;
+	int kop[MAXS], op_hd, op_hi, op_lo;
+	const int nops = stage_ops(sc, S, COMP, demag, kop, op_hd, op_hi, op_lo);
+	// barriers: halo planes arrived [ST_RING], operands arrived [ST_NOB], step done [ST_NOB]
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_st + G::YB + G::RB + ST_NOB * (size_t)nops * G::OPB);
+	uint64_t *bar_o = bar + ST_RING, *bar_done = bar + ST_RING + ST_NOB;
+	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+	constexpr int CONSUMERS = ST_CONS / 32;
+	const int nx = a.nx, ny = a.ny, nz = a.nz;
+	const size_t n = (size_t)nx * ny * nz;
+	if (tid == 0) {
+		for (int b = 0; b < ST_RING + ST_NOB; ++b) mbar_init(&bar[b], 1);
+		for (int b = 0; b < ST_NOB; ++b) mbar_init(&bar_done[b], CONSUMERS);
+		fence_proxy_async();
+		abort_flag = 0;
+		if (op_hd >= 0) opmap[op_hd] = &maps.hd;
+		if (op_hi >= 0) opmap[op_hi] = &maps.hi;
+		if (op_lo >= 0) opmap[op_lo] = &maps.lo;
+		for (int l = 0; l < MAXS; ++l) {
+			fb[l] = (T)(st->h * sc.bn[l]);
+			fe[l] = (T)(st->h * sc.ec[l]);
+		}
+		for (int l = 0; l < MAXS; ++l) {
+			if (kop[l] < 0) continue;
+			const void *p = ktab->k[l];
+			opmap[kop[l]] = &maps.k[0];
+			for (int q = 0; q < MAXS; ++q)
+				if (maps.kptr[q] == p) opmap[kop[l]] = &maps.k[q];
+		}
+	}
+	load_ms_table(a, msr);  // ends with __syncthreads
+	const long long nsteps = (long long)tiles_x * tiles_y * nz;
+	const int L0 = (int)(nsteps * blockIdx.x / gridDim.x), L1 = (int)(nsteps * (blockIdx.x + 1) / gridDim.x);
+	// a step's position: plane z of the column tile at (x0, y0); advanced without divisions
+	struct Pos {
+		int x0, y0, z;
+	};
+	auto advance = [&](Pos &q) {
+		if (++q.z < nz) return;
+		q.z = 0;
+		q.x0 += ST_X;
+		if (q.x0 < nx) return;
+		q.x0 = 0;
+		q.y0 += ST_Y;
+	};
+	Pos start;
+	{
+		const int tile = L0 / nz;
+		start.z = L0 - tile * nz;
+		start.x0 = (tile % tiles_x) * ST_X;
+		start.y0 = (tile / tiles_x) * ST_Y;
+	}
+	// halo planes get consecutive ring indices g (plane g in slot g % ST_RING, its k-th use of the
+	// slot completing phase k); a step that starts a tile (or the CTA's range) loads planes z-1,
+	// z, z+1, a later one plane z+1.  Returns the ring index of plane z; g_next counts the planes.
+	auto plan = [&](const Pos &q, bool first, int &g_next) -> int {
+		int gz;
+		if (first) {
+			if (q.z > 0) ++g_next;
+			gz = g_next++;
+		} else {
+			gz = g_next - 1;
+		}
+		if (q.z + 1 < nz) ++g_next;
+		return gz;
+	};
+	T e2 = T(0), k02 = T(0);
+	int prod_j = 0, prod_g = 0;  // steps and halo planes whose copies the producer issued
+
+	if (warp == CONSUMERS) {
+		// producer: issues step j's copies once step j - ST_NOB (the last reader of the buffers
+		// they overwrite) is done
+		if (lane == 0) {
+			Pos q = start;
+			int g_next = 0;
+			for (int j = 0; L0 + j < L1; ++j, advance(q)) {
+				if (j >= ST_NOB) {
+					const int d = j - ST_NOB;
+					bool ok = false;
+					if (!*(volatile int *)&abort_flag) ok = mbar_wait(&bar_done[d % ST_NOB], (d / ST_NOB) & 1);
+					if (!ok) {
+						*(volatile int *)&abort_flag = 1;
+						break;
+					}
+				}
+				fence_proxy_async();
+				const int g0 = g_next;
+				plan(q, j == 0 || q.z == 0, g_next);
+				for (int g = g0; g < g_next; ++g) {
+					const int p = q.z + 1 - (g_next - 1 - g) - (q.z + 1 < nz ? 0 : 1);
+					uint64_t *b = &bar[g % ST_RING];
+					mbar_expect_tx(b, (uint32_t)(G::YBOX + (a.reg ? G::RBOX : 0)));
+					tma_load_4d(ys + (g % ST_RING) * G::YSLOT, &maps.yin, q.x0 - 4, q.y0 - 1, p, 0, b);
+					if (a.reg) tma_load_3d(rs + (g % ST_RING) * G::RSLOT, &maps.reg, q.x0 - 16, q.y0 - 1, p, b);
+				}
+				const int ob = j % ST_NOB;
+				uint64_t *b = &bar_o[ob];
+				mbar_expect_tx(b, (uint32_t)(nops * G::OPB));
+				for (int k = 0; k < nops; ++k)
+					tma_load_4d(os + (size_t)(ob * nops + k) * 3 * ST_Y * ST_X, opmap[k], q.x0, q.y0, q.z, 0, b);
+				prod_j = j + 1;
+				prod_g = g_next;
+			}
+		}
+	} else {
+		// consumers: ST_CPT cells per thread and step
+		T *const kS = ktab->k[S];
+		const double t = st->t + sc.a_i * st->h;
+		const V3<T> Hz = zeeman_field(a, t);
+		const int lx = tid % ST_X, ly0 = tid / ST_X;  // cells (lx, ly0 + u ST_Y / ST_CPT)
+		const int hc = lx + 4;
+		Pos cur = start;
+		int g_next = 0, g_waited = 0;
+		for (int j = 0; L0 + j < L1; ++j, advance(cur)) {
+			const int z = cur.z, x0 = cur.x0, y0 = cur.y0;
+			const int gz = plan(cur, j == 0 || z == 0, g_next);
+			const int ob = j % ST_NOB;
+			// every lane waits (a completed phase returns at once), so each lane's reads follow
+			// its own observation of the copies
+			bool late = *(volatile int *)&abort_flag != 0;
+			const int g_need = gz + (z + 1 < nz ? 1 : 0);
+			for (; !late && g_waited <= g_need; ++g_waited)
+				late = !mbar_wait(&bar[g_waited % ST_RING], (g_waited / ST_RING) & 1);
+			if (!late) late = !mbar_wait(&bar_o[ob], (j / ST_NOB) & 1);
+			if (__any_sync(0xffffffffu, late)) {
+				if (lane == 0) *(volatile int *)&abort_flag = 1;
+				break;
+			}
+#pragma unroll
+			for (int u = 0; u < ST_CPT; ++u) {
+				const int ly = ly0 + u * (ST_Y / ST_CPT), hr = ly + 1;
+				const int x = x0 + lx, yy = y0 + ly;
+				if (x < nx && yy < ny) {
+					const size_t i = ((size_t)z * ny + yy) * nx + x;
+					// this cell in the ring slots of planes z-1, z, z+1 (component stride YC) and in
+					// the operand buffer (operand stride OS, component stride OC); 32-bit offsets
+					constexpr int YC = ST_YH * ST_XH, OC = ST_Y * ST_X, OS = 3 * OC;
+					const int cell_off = hr * ST_XH + hc;
+					const T *yz = reinterpret_cast<const T *>(ys + (gz % ST_RING) * G::YSLOT) + cell_off;
+					const T *ym = reinterpret_cast<const T *>(ys + ((gz + ST_RING - 1) % ST_RING) * G::YSLOT) + cell_off;
+					const T *yp = reinterpret_cast<const T *>(ys + ((gz + 1) % ST_RING) * G::YSLOT) + cell_off;
+					const int rcell = hr * ST_XR + hc + 12;
+					const uint8_t *rz = rs + (gz % ST_RING) * G::RSLOT + rcell;
+					const uint8_t *rm = rs + ((gz + ST_RING - 1) % ST_RING) * G::RSLOT + rcell;
+					const uint8_t *rp = rs + ((gz + 1) % ST_RING) * G::RSLOT + rcell;
+					const T *oc = os + ob * nops * OS + ly * ST_X + lx;
+					auto O3 = [&](int k) -> V3<T> {
+						const T *o = oc + k * OS;
+						return v3<T>(o[0], o[OC], o[2 * OC]);
+					};
+					auto Y3 = [&](const T *p, int off) -> V3<T> { return v3<T>(p[off], p[off + YC], p[off + 2 * YC]); };
+					const int rg = a.reg ? *rz : 0;
+					const DevMat<T> &M = a.mat[rg < a.nmat ? rg : 0];
+					const V3<T> hd = demag ? O3(op_hd) : v3<T>(0, 0, 0);
+					V3<T> Heff, ki;
+					if (M.Ms == T(0)) {
+						ki = v3<T>(0, 0, 0);
+					} else {
+						const V3<T> m = Y3(yz, 0);
+						const bool has[6] = {x > 0, x < nx - 1, yy > 0, yy < ny - 1, z > 0, z < nz - 1};
+						const T *yq[6] = {yz, yz, yz, yz, ym, yp};
+						const uint8_t *rq[6] = {rz, rz, rz, rz, rm, rp};
+						const int dq[6] = {-1, 1, -ST_XH, ST_XH, 0, 0};
+						const int drq[6] = {-1, 1, -ST_XR, ST_XR, 0, 0};
+						V3<T> nb[6];
+						T nms[6];
+#pragma unroll
+						for (int q = 0; q < 6; ++q) {
+							if (has[q]) {
+								nb[q] = Y3(yq[q], dq[q]);
+								nms[q] = a.reg ? msr[rq[q][drq[q]]] : M.Ms;
+							} else {
+								nb[q] = v3<T>(0, 0, 0);
+								nms[q] = T(0);
+							}
+						}
+						cell_core<T>(a, M, m, nb, nms, x, yy, z, hd, Hz, Heff, ki);
+					}
+					T *const pk = kS + i, *const py = y_out + i;
+					auto put3 = [&](T *p, V3<T> v) {
+						p[0] = v.x;
+						p[n] = v.y;
+						p[2 * n] = v.z;
+					};
+					if (!sc.last) {
+						if (sc.write_next) {
+							V3<T> acc = COMP ? O3(op_lo) : O3(op_hi);
+#pragma unroll
+							for (int l = 0; l < S; ++l) {
+								const T f = fb[l];
+								if (f != T(0)) acc = acc + f * O3(kop[l]);
+							}
+							acc = acc + fb[S] * ki;
+							if (COMP) acc = O3(op_hi) + acc;
+							put3(py, acc);
+						}
+						if (sc.reduce_k0) {
+							const V3<T> k0 = S == 0 ? ki : O3(kop[0]);
+							k02 = max(k02, dot(k0, k0));
+						}
+					} else {
+						V3<T> err = v3<T>(0, 0, 0);
+						V3<T> acc = v3<T>(0, 0, 0);
+#pragma unroll
+						for (int l = 0; l <= S; ++l) {
+							const T fel = fe[l];
+							const T fc = fb[l];
+							if (fel == T(0) && (!sc.write_new || fc == T(0))) continue;
+							const V3<T> kl = l == S ? ki : O3(kop[l]);
+							err = err + fel * kl;
+							if (sc.write_new) acc = acc + fc * kl;
+						}
+						e2 = nan_max(e2, dot(err, err));
+						if (sc.write_new) {
+							if (COMP) {
+								// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
+								const V3<T> hi = O3(op_hi);
+								const V3<T> d = O3(op_lo) + acc;
+								const V3<T> s = hi + d;
+								const V3<T> bb = s - hi;
+								const V3<T> lo = (hi - (s - bb)) + (d - bb);
+								put3(py, s);
+								put3(y_out_lo + i, lo);
+							} else {
+								put3(py, O3(op_hi) + acc);
+							}
+						}
+					}
+					put3(pk, ki);
+				}
+			}
+			__syncwarp();
+			if (lane == 0) mbar_arrive(&bar_done[ob]);
+		}
+	}
+	__syncthreads();  // producer and consumers joined
+	if (warp == CONSUMERS && lane == 0) {
+		// let every copy issued land before the CTA can retire (immediate unless a wait gave up):
+		// wait for the last phase armed on each barrier
+		for (int b = 0; b < ST_NOB && b < prod_j; ++b)
+			mbar_wait(&bar_o[b], ((b + ((prod_j - 1 - b) / ST_NOB) * ST_NOB) / ST_NOB) & 1);
+		for (int sl = 0; sl < ST_RING && sl < prod_g; ++sl)
+			mbar_wait(&bar[sl], ((sl + ((prod_g - 1 - sl) / ST_RING) * ST_RING) / ST_RING) & 1);
+	}
+	if (abort_flag) {
+		if (tid == 0) atomicExch(&st->stage_timeout, 1);
+		return;
+	}
+	if (sc.last) block_max_to(&st->max_err2, e2);
+	if (sc.reduce_k0) block_max_to(&st->max_k02, k02);
+}
+
 // Accepted step: m <- y_{n+1} / |y_{n+1}| (VectorMatrix::normalize to Ms, in unit form).
 template <typename T, bool COMP>
 __device__ __forceinline__ void accept_cell(size_t n, const T *__restrict__ ynew, const T *__restrict__ ynew_lo,
@@ -502,7 +863,7 @@ __device__ __forceinline__ void control_attempt(DevState *st, KTab<T> *ktab, dou
 		h_new = fmin(fmax(h * sc, 1e-15), 1e-10);
 		if (h_new == 1e-15) accept = 1;
 	}
-	const int timed_out = conv_timeout ? *conv_timeout : 0;
+	const int timed_out = (conv_timeout ? *conv_timeout : 0) | st->stage_timeout;
 	if (!finite || timed_out) accept = 0;
 	st->accept = accept;
 	st->h_new = h_new;
@@ -679,6 +1040,12 @@ struct mm_solver {
 	// default stream), ordered after / before the caller's stream with events
 	cudaStream_t gs = nullptr;
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+	// staged stage kernel: used when the rows are 16-byte aligned; grid and shared memory per stage
+	bool st_tma = false;
+	int st_grid[MAXS] = {};
+	size_t st_smem[MAXS] = {};
+	StageMaps st_maps{};             // yin set per launch from st_yin
+	CUtensorMap st_yin[3];           // halo-box maps over m, ys[0], ys[1]
 };
 
 namespace mm {
@@ -873,10 +1240,138 @@ void stage_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc,
 	                                                     (int)tg.x, (int)tg.y, ntiles);
 }
 
+// Coefficients of stage i of an attempt (i = 0: the k_0 evaluation when it is not reused).
+StageCoef stage_coef(const Tableau &tb, int i, bool comp)
+{
+	StageCoef sc{};
+	sc.stage = i;
+	sc.a_i = tb.a[i];
+	if (i == 0) {
+		sc.write_next = 1;
+		sc.bn[0] = tb.b[1][0];
+		return sc;
+	}
+	sc.last = (i == tb.s - 1);
+	sc.reduce_k0 = (i == 1);
+	if (!sc.last) {
+		sc.write_next = 1;
+		for (int l = 0; l <= i; ++l) sc.bn[l] = tb.b[i + 1][l];
+	} else {
+		sc.write_new = comp || !tb.fsal;
+		for (int l = 0; l <= i; ++l) {
+			sc.bn[l] = tb.c[l];
+			sc.ec[l] = tb.ec[l];
+		}
+	}
+	return sc;
+}
+
+template <typename T, bool COMP, int S>
+mm_status stage_tma_prepare(mm_solver *s)
+{
+	using G = StTmaGeom<T>;
+	int kop[MAXS], hd, hi, lo;
+	const StageCoef sc = stage_coef(s->tab, S, COMP);
+	const int nops = stage_ops(sc, S, COMP, (s->cfg.terms & MM_TERM_DEMAG) != 0, kop, hd, hi, lo);
+	const size_t smem = G::smem(nops);
+	int dev = 0, optin = 0;
+	MM_CUDA(cudaGetDevice(&dev));
+	MM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+	if (smem + 2 * 256 * sizeof(T) > (size_t)optin) return fail(MM_ERR_UNSUPPORTED, "staged stage: shared memory");
+	MM_CUDA(cudaFuncSetAttribute(k_stage_tma<T, COMP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                             optin - 2 * 256 * (int)sizeof(T)));
+	int per_sm = 0;
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tma<T, COMP, S>, ST_CONS + 32, smem));
+	if (per_sm < 1) return fail(MM_ERR_UNSUPPORTED, "staged stage kernel does not fit on an SM");
+	const mm_solver_config &c = s->cfg;
+	const long long nsteps = (long long)((c.nx + ST_X - 1) / ST_X) * ((c.ny + ST_Y - 1) / ST_Y) * c.nz;
+	long long grid = std::min<long long>((long long)per_sm * num_sms(), nsteps);
+	// MMB200_STAGE_GRID caps the grid (more steps per CTA; used by the tests)
+	if (const char *cap = std::getenv("MMB200_STAGE_GRID"))
+		if (std::atoi(cap) > 0) grid = std::min<long long>(grid, std::atoi(cap));
+	s->st_grid[S] = (int)grid;
+	s->st_smem[S] = smem;
+	return MM_OK;
+}
+
+// Tensor maps of the staged stage kernel over the solver's buffers.
+template <typename T>
+mm_status stage_tma_maps(mm_solver *s)
+{
+	const mm_solver_config &c = s->cfg;
+	const uint64_t e = sizeof(T);
+	const uint64_t dims[4] = {(uint64_t)c.nx, (uint64_t)c.ny, (uint64_t)c.nz, 3};
+	const uint64_t strides[3] = {c.nx * e, (uint64_t)c.nx * c.ny * e, (uint64_t)s->n * e};
+	const uint32_t hbox[4] = {ST_XH, ST_YH, 1, 3}, obox[4] = {ST_X, ST_Y, 1, 3};
+	StageMaps &m = s->st_maps;
+	const void *yin[3] = {s->m, s->ys[0], s->ys[1]};
+	for (int q = 0; q < 3; ++q) MM_TRY(tma_encode_as(&s->st_yin[q], yin[q], 4, dims, strides, hbox, (int)e));
+	MM_TRY(tma_encode_as(&m.hd, s->hd, 4, dims, strides, obox, (int)e));
+	MM_TRY(tma_encode_as(&m.hi, s->m, 4, dims, strides, obox, (int)e));
+	if (s->m_lo) MM_TRY(tma_encode_as(&m.lo, s->m_lo, 4, dims, strides, obox, (int)e));
+	for (int q = 0; q < MAXS; ++q) {
+		m.kptr[q] = s->k[q];
+		if (s->k[q]) MM_TRY(tma_encode_as(&m.k[q], s->k[q], 4, dims, strides, obox, (int)e));
+	}
+	if (s->reg) {
+		const uint64_t rd[3] = {(uint64_t)c.nx, (uint64_t)c.ny, (uint64_t)c.nz};
+		const uint64_t rs[2] = {(uint64_t)c.nx, (uint64_t)c.nx * c.ny};
+		const uint32_t rb[3] = {ST_XR, ST_YH, 1};
+		MM_TRY(tma_encode_as(&m.reg, s->reg, 3, rd, rs, rb, 1));
+	}
+	return MM_OK;
+}
+
+// Grid and shared memory of the staged stage kernel for every stage of the tableau (at solver
+// creation, so that no later call queries occupancy during stream capture).
+template <typename T, int... S>
+mm_status stage_tma_setup(mm_solver *s, std::integer_sequence<int, S...>)
+{
+	constexpr bool COMP = sizeof(T) == 4;
+	const char *env = std::getenv("MMB200_STAGE_TMA");
+	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr) && !(env && env[0] == '0');
+	if (!s->st_tma) return MM_OK;
+	mm_status r = stage_tma_maps<T>(s);
+	((r = (r == MM_OK && S < s->tab.s) ? stage_tma_prepare<T, COMP, S>(s) : r), ...);
+	if (r != MM_OK) {
+		// a box the tensor-map encoder or the SM does not take: the per-thread-load stage kernel
+		s->st_tma = false;
+		cudaGetLastError();
+	}
+	return MM_OK;
+}
+
+template <typename T, bool COMP, int S>
+void stage_tma_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc, const T *yin, const T *yhi,
+                      const T *ylo, const KTab<T> *kt, T *yout, DevState *ds, cudaStream_t st)
+{
+	const mm_solver_config &c = s->cfg;
+	StageMaps maps = s->st_maps;
+	maps.yin = s->st_yin[yin == (const T *)s->ys[0] ? 1 : (yin == (const T *)s->ys[1] ? 2 : 0)];
+	(void)yhi;
+	(void)ylo;
+	k_stage_tma<T, COMP, S><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+	    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, (c.nx + ST_X - 1) / ST_X, (c.ny + ST_Y - 1) / ST_Y);
+}
+
 template <typename T, bool COMP>
 mm_status launch_stage(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc, const T *yin, const T *yhi,
                        const T *ylo, const KTab<T> *kt, T *yout, DevState *ds, cudaStream_t st)
 {
+	if (s->st_tma) {
+		switch (sc.stage) {
+		case 0: stage_tma_launch<T, COMP, 0>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 1: stage_tma_launch<T, COMP, 1>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 2: stage_tma_launch<T, COMP, 2>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 3: stage_tma_launch<T, COMP, 3>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 4: stage_tma_launch<T, COMP, 4>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 5: stage_tma_launch<T, COMP, 5>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 6: stage_tma_launch<T, COMP, 6>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		case 7: stage_tma_launch<T, COMP, 7>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
+		default: return fail(MM_ERR_INVALID_ARGUMENT, "stage index beyond the supported tableau size");
+		}
+		return after_launch("k_stage_tma");
+	}
 	switch (sc.stage) {
 	case 0: stage_launch<T, COMP, 0>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
 	case 1: stage_launch<T, COMP, 1>(s, a, sc, yin, yhi, ylo, kt, yout, ds, st); break;
@@ -921,11 +1416,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 	const KTab<T> *kt = (const KTab<T> *)s->ktab;
 	T *ys[2] = {(T *)s->ys[0], (T *)s->ys[1]};
 	if (eval_k0) {
-		StageCoef sc{};
-		sc.stage = 0;
-		sc.a_i = tb.a[0];
-		sc.write_next = 1;
-		sc.bn[0] = tb.b[1][0];
+		const StageCoef sc = stage_coef(tb, 0, COMP);
 		MM_TRY(demag<T>(s, s->m, st));
 		ProfToken tk = prof_begin(st);
 		MM_TRY((launch_stage<T, COMP>(s, a, sc, yhi, yhi, ylo, kt, ys[0], ds, st)));
@@ -938,21 +1429,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		prof_end(tk, "k_prepare1", (double)n3 * sizeof(T) * (COMP ? 4 : 3), st);
 	}
 	for (int i = 1; i < tb.s; ++i) {
-		StageCoef sc{};
-		sc.stage = i;
-		sc.last = (i == tb.s - 1);
-		sc.a_i = tb.a[i];
-		sc.reduce_k0 = (i == 1);
-		if (!sc.last) {
-			sc.write_next = 1;
-			for (int l = 0; l <= i; ++l) sc.bn[l] = tb.b[i + 1][l];
-		} else {
-			sc.write_new = COMP || !tb.fsal;
-			for (int l = 0; l <= i; ++l) {
-				sc.bn[l] = tb.c[l];
-				sc.ec[l] = tb.ec[l];
-			}
-		}
+		const StageCoef sc = stage_coef(tb, i, COMP);
 		const T *yin = ys[(i - 1) & 1];
 		MM_TRY(demag<T>(s, yin, st));
 		ProfToken tk = prof_begin(st);
@@ -1192,6 +1669,7 @@ mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uin
 		MM_TRY(r);
 	}
 	stage_resident<T, sizeof(T) == 4>();
+	MM_TRY(stage_tma_setup<T>(s, std::make_integer_sequence<int, MAXS>()));
 	MM_CUDA(cudaStreamSynchronize(st));
 	return MM_OK;
 }

@@ -20,6 +20,9 @@ mm_status tma_encode_3d(CUtensorMap *map, const void *base, uint64_t d0, uint64_
 // Same for rank 1..5: dims[0] fastest, strides[] in bytes of dims 1..rank-1.
 mm_status tma_encode(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
                      const uint32_t *box);
+// Same with elements of esize bytes (1, 4 or 8; copied as unsigned integers of that size).
+mm_status tma_encode_as(CUtensorMap *map, const void *base, int rank, const uint64_t *dims, const uint64_t *strides,
+                        const uint32_t *box, int esize);
 
 // Spin limit of a bounded mbarrier wait (each try_wait already blocks for a while in hardware);
 // a wait that exceeds it reports a timeout instead of hanging the GPU.
@@ -46,6 +49,12 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
 {
 	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
 	             : "memory");
+}
+
+// Plain arrival (no transaction bytes).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
 // Bounded wait for the phase with the given parity to complete; false on timeout.
@@ -85,6 +94,16 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, i
 	    "%5}], [%6];" ::"r"(smem_u32(dst)),
 	    "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
 	    : "memory");
+}
+
+// Untiled bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global
+// into this CTA's shared memory, completing on `bar` (transaction bytes).
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+	                 smem_u32(dst)),
+	             "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+	             : "memory");
 }
 
 // 3-D tiled load of one box into shared memory, completing on `bar` (transaction bytes).

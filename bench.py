@@ -265,6 +265,17 @@ def run_ours(args, rank, world, local_rank):
         with open(tpath) as f:
             traffic = json.load(f).get(name)
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
+    tfile = {}
+    if os.path.exists(tpath):
+        with open(tpath) as f:
+            tfile = json.load(f)
+
+    def kernel_roofline(k):
+        c, t_ms, b = prof[k]
+        a = (b / c) / (t_ms / c * 1e-3) / 1e9
+        return {"bound": "hbm", "kernel": k, "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
+                "peak_kind": peak_kind, "traffic": tfile.get(k), "algorithmic_bytes_per_launch": b / c,
+                "launch_ms": t_ms / c}
 
     # ---- end to end through the public API with host buffers -----------------------------------
     h_in = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
@@ -305,6 +316,7 @@ def run_ours(args, rank, world, local_rank):
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": tot_bytes / cnt, "launch_ms": tot_ms / cnt,
                          "time_shares": shares},
+            "stage_roofline": kernel_roofline("k_stage") if "k_stage" in prof else None,
             "cpu_baseline": cpu,
             "clocks": clk,
         }

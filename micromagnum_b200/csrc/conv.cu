@@ -1616,6 +1616,7 @@ template <typename T>
 struct GDesc {
 	cplx<T> *spec;
 	const T *tensor;
+	const T *tensor_t;  // fused y+z members: the reduced tensor kx-major, [hx][qz][qy][6]
 	const cplx<T> *tw_x, *tw_y;
 	const T *M[3];
 	T *H;
@@ -1798,6 +1799,22 @@ __device__ __forceinline__ void cp_async_wait_all_c() { asm volatile("cp.async.w
 // Lines are split into G groups of LG lines so that a group's transform needs at most 512 threads
 // (128 registers per thread for the z columns); tiles stay within ~104 KB of shared memory so
 // that two CTAs share an SM.
+// Reduced tensor [6][qz][qy][hx] -> kx-major [hx][qz][qy][6] (one thread per destination entry).
+template <typename T>
+__global__ void k_tensor_kx(const T *__restrict__ src, T *__restrict__ dst, int hx, int qy, int qz)
+{
+	const size_t ne = (size_t)6 * hx * qy * qz;
+	for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < ne; e += (size_t)gridDim.x * blockDim.x) {
+		const int c = (int)(e % 6);
+		size_t r = e / 6;
+		const int ky = (int)(r % qy);
+		r /= qy;
+		const int kz = (int)(r % qz);
+		const int kx = (int)(r / qz);
+		dst[e] = src[(((size_t)c * qz + kz) * qy + ky) * hx + kx];
+	}
+}
+
 template <int PY, int PZ, class C>
 struct YZGeom {
 	static constexpr int NZ = PZ / 2;  // planes a member of this group can have (nz <= pz/2)
@@ -1858,7 +1875,6 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 	}
 	__syncthreads();
 	// z transforms, tensor multiply, inverse z transforms: one thread per (ky, column)
-	const size_t cs = (size_t)g.qz * g.qy * hx, kzs = (size_t)g.qy * hx;
 	for (int item = tid; item < PY * TB; item += G::THREADS) {
 		const int col = item % TB, ky = item / TB;
 		const int kx = kx0 + col;
@@ -1875,10 +1891,13 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 		const T sy = fy ? T(-1) : T(1);
 		// kz and PZ - kz share the tensor entries (sign of the z-odd components flipped): each
 		// reduced entry is loaded once
+		using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
 #pragma unroll
 		for (int kzr = 0; kzr <= H; ++kzr) {
-			const T *t = g.tensor + (size_t)kzr * kzs + (size_t)kyr * hx + kx;
-			const T nxx = t[0], nxy = t[cs], nxz = t[2 * cs], nyy = t[3 * cs], nyz = t[4 * cs], nzz = t[5 * cs];
+			// the six components of entry (kx, kzr, kyr), contiguous (8- or 16-byte aligned pairs)
+			const T2 *t = reinterpret_cast<const T2 *>(g.tensor_t + (((size_t)kx * g.qz + kzr) * g.qy + kyr) * 6);
+			const T2 t0 = t[0], t1 = t[1], t2 = t[2];
+			const T nxx = t0.x, nxy = t0.y, nxz = t1.x, nyy = t1.y, nyz = t2.x, nzz = t2.y;
 #pragma unroll
 			for (int q = 0; q < ((kzr == 0 || kzr == H) ? 1 : 2); ++q) {
 				const int p = brev<PZ>(q ? PZ - kzr : kzr);
@@ -1938,6 +1957,7 @@ struct ConvGroup {
 	CUtensorMap *maps = nullptr;  // [2 member + inverse]: spectrum views of the y passes
 	bool maps_ok = false;         // every member's maps exist (variant 3 possible)
 	int *err = nullptr;           // set when a staged pass gave up waiting
+	std::vector<void *> owned;    // kx-major tensors of the fused members
 	// the lists of one phase (independent members) run side by side on these streams
 	static constexpr int POOL = 8;
 	cudaStream_t pool[POOL] = {};
@@ -1947,6 +1967,7 @@ struct ConvGroup {
 		cudaFree(desc);
 		cudaFree(maps);
 		cudaFree(err);
+		for (void *q : owned) cudaFree(q);
 		for (auto &l : lists) cudaFree(l.items);
 		for (auto &q : pool)
 			if (q) cudaStreamDestroy(q);
@@ -2000,16 +2021,30 @@ void with_yz(int key, F &&f)
 
 // Whether a member takes the fused y+z pass (and its columns per CTA).
 template <typename T>
-int yz_tb(const ConvPlan *p)
+int yz_tb_dims(int py, int pz, int nz)
 {
 	int tb = 0;
-	if (p->py < 16 || p->py > 512 || (p->pz != 2 && p->pz != 4 && p->pz != 8) || 2 * p->nz > p->pz) return 0;
-	with_yz(p->py * 64 + p->pz, [&](auto pyc, auto pzc) {
+	if (py < 16 || py > 512 || (pz != 2 && pz != 4 && pz != 8) || 2 * nz > pz) return 0;
+	with_yz(py * 64 + pz, [&](auto pyc, auto pzc) {
 		using G = YZGeom<decltype(pyc)::value, decltype(pzc)::value, cplx<T>>;
 		if constexpr (G::fits) tb = G::TB;
 	});
 	return tb;
 }
+template <typename T>
+int yz_tb(const ConvPlan *p)
+{
+	return yz_tb_dims<T>(p->py, p->pz, p->nz);
+}
+
+} // namespace
+
+int conv_group_fused(int prec, int py, int pz, int nz)
+{
+	return prec == MM_F32 ? yz_tb_dims<float>(py, pz, nz) > 0 : yz_tb_dims<double>(py, pz, nz) > 0;
+}
+
+namespace {
 
 // Threads of one CTA of a pass/length/variant (0 when the variant does not exist).
 template <typename T>
@@ -2284,9 +2319,18 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		d.flags = nullptr;  // the autotuner runs every member; the real flags are set below
 		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
 		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
+		d.tensor_t = nullptr;
 		lists[{0, p->px}].push_back(i);
 		if (yz_tb<T>(p) > 0) {
 			lists[{6, p->py * 64 + p->pz}].push_back(i);  // y, z and the multiply in one pass
+			// the fused pass reads the tensor by (kx, kz, ky) with its six components together
+			T *tt = nullptr;
+			const size_t ne = (size_t)6 * p->hx * p->qy * p->qz;
+			MM_CUDA(cudaMalloc(&tt, ne * sizeof(T)));
+			g->owned.push_back(tt);
+			k_tensor_kx<T><<<(unsigned)((ne + 255) / 256), 256, 0, st>>>((const T *)p->tensor, tt, p->hx, p->qy, p->qz);
+			MM_CUDA(cudaGetLastError());
+			d.tensor_t = tt;
 		} else {
 			lists[{1, p->py}].push_back(i);
 			lists[{2, p->pz}].push_back(i);

@@ -79,6 +79,9 @@ mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int
 mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st);
 int conv_group_launches(const ConvGroup *g);
 void conv_group_destroy(ConvGroup *g);
+// Whether a member with these padded lengths takes the grouped fused y+z pass (which keeps a
+// second, kx-major copy of its reduced tensor).
+int conv_group_fused(int prec, int py, int pz, int nz);
 
 FftRadices fft_factor(int n);
 

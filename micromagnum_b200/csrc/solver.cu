@@ -2381,7 +2381,9 @@ void instance_bytes(const mm_batch_instance &q, int prec, size_t *resident, size
 	w = (w + 2 * nb - 1) / (2 * nb) * (2 * nb);
 	const size_t lx = w / E;
 	const size_t vecs = (prec == MM_F32 ? 3 : 1) + 2 + 7 + 1;  // m (+lo, ynew_lo), ys[2], k[7], H_demag
-	*resident = vecs * 3 * n * s + n + 3 * (size_t)q.nz * py * lx * 2 * s + 6 * qz * qy * hx * s + (1 << 16);
+	const size_t tensor = 6 * qz * qy * hx * s;
+	*resident = vecs * 3 * n * s + n + 3 * (size_t)q.nz * py * lx * 2 * s + tensor + (1 << 16);
+	if (conv_group_fused(prec, py, pz, q.nz)) *resident += tensor;  // the fused pass's kx-major copy
 	*transient = 6 * (size_t)px * py * pz * 8 + (size_t)px * py * pz * 16;
 }
 

@@ -55,6 +55,7 @@ class ServeStats:
     rounds: int = 0
     peak_resident: int = 0
     unfinished: int = 0  # requests not finished when the deadline passed
+    progress: dict = field(default_factory=dict)  # request id -> accepted steps made (admitted requests)
 
     def percentile(self, q: float) -> float:
         return float(np.percentile([c.latency for c in self.completed], q)) if self.completed else float("nan")
@@ -168,7 +169,13 @@ class Server:
         for th in threads:
             th.join()
         stats.makespan = clock() - t0
+        for c in stats.completed:
+            stats.progress[c.id] = c.steps
         for cl in self.classes:
+            if cl.live:
+                res = cl.batch.results()
+                for slot, (req, _, _) in cl.live.items():
+                    stats.progress[req.id] = res[slot]["steps"]
             for slot in list(cl.live):
                 cl.batch.remove(slot)
             cl.live.clear()

@@ -636,10 +636,15 @@ __device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__r
 	// the block's tensor entries (kz' <= pz/2, 6 components, 32 kx at ky' = b) come in by
 	// asynchronous copies while the columns are loaded and transformed
 	T *tens = reinterpret_cast<T *>(sm + 2 * PZ * 96);
-	const size_t cs = (size_t)qz * qy * hx, kzs = (size_t)qy * hx;
-	for (int e = threadIdx.x; e < (H + 1) * 6 * 32; e += ZR_THREADS) {
-		const int kzr = e / 192, comp = (e / 32) % 6, kxx = bx * 32 + (e & 31);
-		if (kxx < hx) cp_async_t(&tens[e], Nt + comp * cs + kzr * kzs + (size_t)b * hx + kxx);
+	static_assert(ZR_THREADS == 192, "one thread per (tensor component, kx) of a kz plane");
+	{
+		// thread (warp w, lane) copies component w at kx for every kz' (one pointer step per plane)
+		const size_t kzs = (size_t)qy * hx;
+		const T *src = Nt + (size_t)w * qz * kzs + (size_t)b * hx + kx;
+		if (kx < hx) {
+#pragma unroll
+			for (int kzr = 0; kzr <= H; ++kzr, src += kzs) cp_async_t(&tens[kzr * 192 + threadIdx.x], src);
+		}
 	}
 	C v[PZ];
 #pragma unroll
@@ -655,8 +660,12 @@ __device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__r
 			const T *t = tens + kzr * 192 + lane;
 			const T nxx = t[0], nxy = t[32], nxz = t[64], nyy = t[96], nyz = t[128], nzz = t[160];
 			const int nk = (kzr == 0 || kzr == H) ? 1 : 2;
-			for (int rr = 0; rr < (two ? 2 : 1); ++rr) {
-				for (int q = 0; q < nk; ++q) {
+#pragma unroll
+			for (int rr = 0; rr < 2; ++rr) {
+				if (rr && !two) break;
+#pragma unroll
+				for (int q = 0; q < 2; ++q) {
+					if (q && nk < 2) break;
 					const int kz = q ? PZ - kzr : kzr;
 					const T sy = rr ? T(-1) : T(1), sz = q ? T(-1) : T(1);
 					C *e = sm + ((rr * PZ + kz) * 3) * 32 + lane;

@@ -439,7 +439,7 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2) k_y_ct(cplx<T> *__r
 }
 
 // x pass forward: LPB complex lines per CTA (line q packs real rows 2q, 2q+1).
-template <typename T, int N, int LPB, bool SCALE, int R = ct_radix(N)>
+template <typename T, int N, int LPB, bool SCALE, int R = ct_radix(N), bool H0 = false>
 __device__ __forceinline__ void x_fwd_ct_body(const T *__restrict__ M, const uint8_t *__restrict__ reg,
                                               const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny,
                                               int nz, int py, int hx, int lx, const cplx<T> *__restrict__ twN, int blk)
@@ -467,7 +467,8 @@ __device__ __forceinline__ void x_fwd_ct_body(const T *__restrict__ M, const uin
 		return C{a, b};
 	};
 	auto st = [&](int l, int k, C v) { sm[SI::at(l, k)] = v; };
-	cta_fft<T, N, R, LPB, false, SI>(sm, twN, line, j0, ld, st);
+	if constexpr (H0) cta_fft_h0<T, N, R, LPB, SI>(sm, twN, line, j0, ld, st);
+	else cta_fft<T, N, R, LPB, false, SI>(sm, twN, line, j0, ld, st);
 	__syncthreads();
 	C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
 	C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
@@ -792,7 +793,8 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 				issue(next, b);
 			}
 		};
-		cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
+		if constexpr (INV) cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
+		else cta_fft_h0<T, N, R, TB, SI>(work, twN, line, j0, ld, st, release);  // rows >= N/2 are zero
 	}
 }
 
@@ -879,7 +881,7 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 			return C{a, bb};
 		};
 		auto st = [&](int l, int kk, C v) { sm[SI::at(l, kk)] = v; };
-		cta_fft<T, N, G::R, LPB, false, SI, true>(sm, twN, line, j0, ld, st);
+		cta_fft_h0<T, N, G::R, LPB, SI, true>(sm, twN, line, j0, ld, st);  // x >= nx, N/2 <= x: zero
 		__syncthreads();
 		C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
 		C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
@@ -1043,7 +1045,8 @@ mm_status fs_setup_x_tma(ConvPlan *p)
 	using G = XTmaGeom<N, C>;
 	constexpr int LPB = G::LPB;
 	p->tma_xf = p->tma_xi = false;
-	if (G::SMEM > 227 * 1024 || N < 64) return MM_OK;
+	// the forward pass's half-zero first butterflies need nx <= N/2 (non-periodic zero padding)
+	if (G::SMEM > 227 * 1024 || N < 64 || 2 * p->nx > N) return MM_OK;
 	int occ = 0;
 	// forward: dense real rows split into boxes of even width
 	const size_t wf = (size_t)p->nx * sizeof(T) / 8;
@@ -1662,7 +1665,7 @@ __global__ void __launch_bounds__(LPB * (N / R)) k_x_fwd_grp(const GDesc<T> *__r
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
-	x_fwd_ct_body<T, N, LPB, true, R>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx,
+	x_fwd_ct_body<T, N, LPB, true, R, true>(g.M[input], g.reg, g.ms_tab, g.spec, g.nx, g.ny, g.nz, g.py, g.hx, g.lx,
 	                                  g.tw_x, it.y);
 }
 
@@ -1780,7 +1783,8 @@ __global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)),
 				issue(t2, b);
 			}
 		};
-		cta_fft<T, N, R, TB, INV, SI>(work, g.tw_y, line, j0, ld, st, release);
+		if constexpr (INV) cta_fft<T, N, R, TB, INV, SI>(work, g.tw_y, line, j0, ld, st, release);
+		else cta_fft_h0<T, N, R, TB, SI>(work, g.tw_y, line, j0, ld, st, release);
 		t = t1;
 		t1 = t2;
 	}
@@ -1880,7 +1884,7 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 		C *sm = smem + (size_t)grp * G::GROUP_ELEMS;
 		auto ld = [&](int ll, int y) -> C { return y < ny ? sm[SI::at(ll, y)] : C{0, 0}; };
 		auto st = [&](int ll, int k, C v) { sm[SI::at(ll, k)] = v; };
-		cta_fft<T, PY, G::R, LG, false, SI, true>(sm, g.tw_y, line, j0, ld, st);
+		cta_fft_h0<T, PY, G::R, LG, SI, true>(sm, g.tw_y, line, j0, ld, st);  // rows ny <= PY/2 .. are zero
 	}
 	__syncthreads();
 	// z transforms, tensor multiply, inverse z transforms: one thread per (ky, column)
@@ -2316,6 +2320,8 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		const ConvPlan *p = m[i].plan;
 		if (!p || p->prec != g->prec || p->is2d || !p->fast_x || !p->fast_y || !p->reg_z)
 			return fail(MM_ERR_UNSUPPORTED, "conv group: every member needs power-of-two 3-D padding with a register z pass");
+		if (2 * p->nx > p->px || 2 * p->ny > p->py || 2 * p->nz > p->pz)
+			return fail(MM_ERR_UNSUPPORTED, "conv group: every member needs zero padding to at least twice its size");
 		GDesc<T> &d = h[i];
 		d.spec = (cplx<T> *)p->spec;
 		d.tensor = (const T *)p->tensor;

@@ -127,8 +127,10 @@ struct NoHook {
 	__device__ __forceinline__ void operator()() const {}
 };
 
-template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, class LD, class ST,
-          class HK = NoHook>
+// H0: the inputs at k >= N/2 are zero (a forward transform of zero-padded data), so pass 0 loads
+// only the lower half of each butterfly's inputs and runs the half-zero register DFT.
+template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM, int p, bool H0, class LD,
+          class ST, class HK = NoHook>
 __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0,
                                              LD &ld, ST &st, HK hk = HK())
 {
@@ -139,13 +141,15 @@ __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restr
 	constexpr int TPL = N / R;
 	constexpr int BPT = R / Rp;
 	constexpr int M = N / Rp;                  // butterflies per line, input stride
+	constexpr bool HALF = H0 && p == 0;
+	static_assert(!HALF || (!INV && BPT == 1 && Rp >= 2), "half-zero pass 0: forward, one butterfly per thread");
 	C v[BPT][Rp];
 	if constexpr (p > 0) __syncthreads();
 #pragma unroll
 	for (int u = 0; u < BPT; ++u) {
 		const int j = j0 + u * TPL;
 #pragma unroll
-		for (int q = 0; q < Rp; ++q) {
+		for (int q = 0; q < (HALF ? Rp / 2 : Rp); ++q) {
 			if constexpr (p == 0) v[u][q] = ld(line, j + q * M);
 			else v[u][q] = sm[SmIdx::at(line, j + q * M)];
 		}
@@ -165,7 +169,8 @@ __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restr
 				}
 			}
 		}
-		dft_reg<T, Rp, INV>(v[u]);
+		if constexpr (HALF) dft_reg_halfzero<T, Rp>(v[u]);
+		else dft_reg<T, Rp, INV>(v[u]);
 		const int base = (j / Ns) * Ns * Rp + jm;
 #pragma unroll
 		for (int k = 0; k < Rp; ++k) {
@@ -175,7 +180,8 @@ __device__ __forceinline__ void cta_fft_pass(cplx<T> *sm, const cplx<T> *__restr
 		}
 	}
 	if constexpr (p == 0) hk();
-	if constexpr (p + 1 < P) cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, p + 1>(sm, twN, line, j0, ld, st, hk);
+	if constexpr (p + 1 < P)
+		cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, p + 1, false>(sm, twN, line, j0, ld, st, hk);
 }
 
 // LD_SM: the loader reads the same shared memory the passes write (adds a barrier after pass 0's
@@ -185,7 +191,16 @@ template <typename T, int N, int R, int LANES, bool INV, class SmIdx, bool LD_SM
 __device__ __forceinline__ void cta_fft(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0, LD &ld,
                                         ST &st, HK hk = HK())
 {
-	cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, 0>(sm, twN, line, j0, ld, st, hk);
+	cta_fft_pass<T, N, R, LANES, INV, SmIdx, LD_SM, 0, false>(sm, twN, line, j0, ld, st, hk);
+}
+
+// Forward transform whose inputs at k >= N/2 are zero (ld is not called for them).
+template <typename T, int N, int R, int LANES, class SmIdx, bool LD_SM = false, class LD, class ST,
+          class HK = NoHook>
+__device__ __forceinline__ void cta_fft_h0(cplx<T> *sm, const cplx<T> *__restrict__ twN, int line, int j0, LD &ld,
+                                           ST &st, HK hk = HK())
+{
+	cta_fft_pass<T, N, R, LANES, false, SmIdx, LD_SM, 0, true>(sm, twN, line, j0, ld, st, hk);
 }
 
 } // namespace mm

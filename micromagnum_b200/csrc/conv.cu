@@ -719,7 +719,7 @@ struct YTmaGeom {
 	static constexpr int NBOX = ROWS / BR;
 	static constexpr int E = (int)(sizeof(C) / 8);
 	static constexpr uint32_t TILE_BYTES = (uint32_t)(TB * ROWS * sizeof(C));
-	static constexpr size_t WORK = ((size_t)SmCols<N, TB>::SIZE * sizeof(C) + 15) / 16 * 16;
+	static constexpr size_t WORK = ((size_t)SmCols<N, TB, 4>::SIZE * sizeof(C) + 15) / 16 * 16;
 	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
 };
 
@@ -740,7 +740,7 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 	using C = cplx<T>;
 	using G = YTmaGeom<N, TB, INV, C>;
 	constexpr int R = ct_radix(N);
-	using SI = SmCols<N, TB>;
+	using SI = SmCols<N, TB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
 	C *stage0 = reinterpret_cast<C *>(smem_tma);
 	C *stage1 = stage0 + TB * G::ROWS;
@@ -808,7 +808,7 @@ struct XTmaGeom {
 	static constexpr int R = ct_radix(N);
 	static constexpr int LPB = ct_lpb(N, sizeof(C));
 	static constexpr int THREADS = LPB * (N / R);
-	static constexpr size_t WORK = (size_t)SmRows<N, LPB>::SIZE * sizeof(C);
+	static constexpr size_t WORK = (size_t)SmRows<N, LPB, 4>::SIZE * sizeof(C);
 	// staged rows (at most 2 LPB spectrum rows of N/2 + 1 + padding complex values) fit in WORK
 	// with room to spare for N >= 64; shorter rows use the non-staged kernels
 	static constexpr size_t BUF = (WORK + 127) / 128 * 128;
@@ -828,7 +828,7 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 	using C = cplx<T>;
 	using G = XTmaGeom<N, C>;
 	constexpr int LPB = G::LPB, TPL = N / G::R;
-	using SI = SmRows<N, LPB>;
+	using SI = SmRows<N, LPB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
 	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
 	T *msr = reinterpret_cast<T *>(smem_tma + 2 * G::BUF + 16);
@@ -908,7 +908,7 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 	using C = cplx<T>;
 	using G = XTmaGeom<N, C>;
 	constexpr int LPB = G::LPB, TPL = N / G::R;
-	using SI = SmRows<N, LPB>;
+	using SI = SmRows<N, LPB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
 	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
 	const int tid = threadIdx.x;
@@ -1714,7 +1714,7 @@ __global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)),
 	constexpr int TB = ct_tb(N, sizeof(C));
 	using G = YTmaGeom<N, TB, INV, C>;
 	constexpr int R = ct_radix(N);
-	using SI = SmCols<N, TB>;
+	using SI = SmCols<N, TB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
 	C *stage0 = reinterpret_cast<C *>(smem_tma);
 	C *stage1 = stage0 + TB * G::ROWS;

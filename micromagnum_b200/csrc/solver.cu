@@ -2001,7 +2001,7 @@ constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
 // K0: the k_0 evaluation of instances that need it (others skip it).
 template <typename T, bool COMP, int S, bool TORQUE>
-__global__ void __launch_bounds__(256, stage_min_blocks<T>())
+__global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
     k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items)
 {
 	const int2 it = items[blockIdx.x];
@@ -2014,9 +2014,7 @@ __global__ void __launch_bounds__(256, stage_min_blocks<T>())
 	__syncthreads();
 	load_ms_table(a, msr);
 	const T *y_in = in == 0 ? g.m : g.ys[in - 1];
-	T *K[MAXS];
-#pragma unroll
-	for (int l = 0; l < MAXS; ++l) K[l] = g.kt->k[l];
+	T *const *K = g.kt->k;  // read per use (cached), not held in registers
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
 	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
 		stage_tile<T, COMP, S, TORQUE>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds, it.y + k,

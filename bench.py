@@ -86,9 +86,12 @@ def read_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms; the samples whose own
+    nvidia-smi timestamp falls in the timed region (widened by one interval on each side) are
+    kept, so pipe buffering of nvidia-smi's output cannot move a sample in or out of it."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    INTERVAL_MS = 50
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -102,7 +105,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", str(self.INTERVAL_MS)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except (OSError, FileNotFoundError):
             self.proc = None
             return
@@ -117,13 +120,23 @@ class ClockSampler:
             self.lines.append((time.time(), line.strip()))
 
     def mark(self):
-        """Start of the timed region; samples from 0.5 s before it on are kept (a short timed
-        region may fall between two 200 ms samples)."""
-        self.t_mark = time.time() - 0.5
+        """Start of the timed region."""
+        self.t_mark = time.time()
+
+    @staticmethod
+    def _when(stamp):
+        """nvidia-smi's local-time stamp 'YYYY/MM/DD HH:MM:SS.mmm' as seconds since the epoch."""
+        import datetime
+        try:
+            return datetime.datetime.strptime(stamp, "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
 
     def stop(self):
+        t_end = time.time()
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(2 * self.INTERVAL_MS / 1000.0)  # the sample just after the region
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -133,19 +146,23 @@ class ClockSampler:
             self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        t_mark = getattr(self, "t_mark", 0.0)
+        pad = self.INTERVAL_MS / 1000.0
+        lo, hi = getattr(self, "t_mark", 0.0) - pad, t_end + pad
         for ts, ln in self.lines:
-            if ts < t_mark:
-                continue
             f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
+                continue
+            when = self._when(f[0])
+            if when is None:
+                when = ts  # unparsable stamp: fall back to the read time
+            if not lo <= when <= hi:
                 continue
             try:
-                sm.append(float(f[1]))
-                smax.append(float(f[2]))
+                sm.append(float(f[2]))
+                smax.append(float(f[3]))
             except ValueError:
                 continue
-            for nm, v in zip(names, f[5:9]):
+            for nm, v in zip(names, f[6:10]):
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,

@@ -1868,13 +1868,30 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
 	auto elem = [&](int l, int k) -> C & { return smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, k)]; };
 	// the tile's x-transformed rows (y < ny) land in the groups' buffers by asynchronous copies
 	// issued all at once; lines outside the member (z >= nz, kx >= hx) are never stored
-	for (int e = tid; e < 3 * NZ * TB * ny; e += G::THREADS) {
-		const int col = e % TB, rest = e / TB, y = rest % ny, cz = rest / ny, c = cz / NZ, z = cz % NZ;
-		const int kx = kx0 + col;
-		if (z >= nz || kx >= hx) continue;
-		const int l = cz * TB + col;
-		cp_async_c(&smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, y)],
-		           g.spec + ((size_t)(c * nz + z) * g.py + y) * lx + kx);
+	{
+		// a thread keeps its column and walks the (component-plane, row) pairs, y fastest, with
+		// the row position carried forward instead of divided out per element
+		static_assert(G::THREADS % TB == 0, "a thread keeps its column");
+		constexpr int STEP = G::THREADS / TB;
+		const int col = tid % TB, kx = kx0 + col, rows = 3 * NZ * ny;
+		int row = tid / TB, cz = row / ny, y = row - cz * ny;
+		if (kx < hx) {
+			while (row < rows) {
+				const int c = cz / NZ, z = cz % NZ;
+				if (z < nz) {
+					const int l = cz * TB + col;
+					cp_async_c(&smem[(size_t)(l / LG) * G::GROUP_ELEMS + SI::at(l % LG, y)],
+					           g.spec + ((size_t)(c * nz + z) * g.py + y) * lx + kx);
+				}
+				row += STEP;
+				if (row >= rows) break;
+				y += STEP;
+				while (y >= ny) {
+					y -= ny;
+					++cz;
+				}
+			}
+		}
 	}
 	cp_async_wait_all_c();
 	__syncthreads();

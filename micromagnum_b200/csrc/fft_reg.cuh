@@ -111,14 +111,14 @@ __host__ __device__ constexpr int fft_radix(int N, int R, int p)
 // (stride R) and the column tiles across the banks.  SH = 4 makes the radix-16 pass-0 writes of
 // 8-byte elements conflict-free (consecutive butterflies 17 elements = 34 words apart, so a
 // half-warp's 16 stores cover all 32 banks once); SH = 5 halves the padding.
-template <int SH = 4>
+template <int SH = 5>
 __host__ __device__ constexpr int sm_pad(int raw) { return raw + (raw >> SH); }
-template <int N, int LANES, int SH = 4>
+template <int N, int LANES, int SH = 5>
 struct SmCols {  // element (line, k) at k * LANES + line: lines are adjacent columns
 	static constexpr int SIZE = N * LANES + (N * LANES >> SH) + 1;
 	__device__ __forceinline__ static int at(int line, int k) { return sm_pad<SH>(k * LANES + line); }
 };
-template <int N, int LANES, int SH = 4>
+template <int N, int LANES, int SH = 5>
 struct SmRows {  // element (line, k) at line * N + k
 	static constexpr int SIZE = N * LANES + (N * LANES >> SH) + 1;
 	__device__ __forceinline__ static int at(int line, int k) { return sm_pad<SH>(line * N + k); }

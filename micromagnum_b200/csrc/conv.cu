@@ -772,7 +772,10 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 		const int b = k & 1;
 		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
 		if (__syncthreads_or(late)) {
-			if (tid == 0) atomicExch(err, 1);
+			if (tid == 0) {
+				atomicExch(err, 1);
+				mbar_drain2(bar, parity, b, t + (int)gridDim.x < ntiles);
+			}
 			return;
 		}
 		parity ^= 1u << b;
@@ -860,7 +863,10 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 		const int b = k & 1;
 		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
 		if (__syncthreads_or(late)) {
-			if (tid == 0) atomicExch(err, 1);
+			if (tid == 0) {
+				atomicExch(err, 1);
+				mbar_drain2(bar, parity, b, t + (int)gridDim.x < ntiles);
+			}
 			return;
 		}
 		parity ^= 1u << b;
@@ -935,7 +941,10 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 		const int b = k & 1;
 		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
 		if (__syncthreads_or(late)) {
-			if (tid == 0) atomicExch(err, 1);
+			if (tid == 0) {
+				atomicExch(err, 1);
+				mbar_drain2(bar, parity, b, t + (int)gridDim.x < ntiles);
+			}
 			return;
 		}
 		parity ^= 1u << b;
@@ -1758,7 +1767,10 @@ __global__ void __launch_bounds__(ct_tb(N, sizeof(cplx<T>)) * (N / ct_radix(N)),
 		const int b = k & 1;
 		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
 		if (__syncthreads_or(late)) {
-			if (tid == 0) atomicExch(err, 1);
+			if (tid == 0) {
+				atomicExch(err, 1);
+				mbar_drain2(bar, parity, b, t1 < n_items);
+			}
 			return;
 		}
 		parity ^= 1u << b;

@@ -75,6 +75,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 	return false;
 }
 
+// After a bounded wait gave up in a two-buffer pipeline: waits (bounded again) for the loads
+// still in flight, the one that timed out on buffer b and, when one was issued, the next one on
+// the other buffer, so that no copy lands in shared memory after the CTA has exited.
+__device__ __forceinline__ void mbar_drain2(uint64_t *bar, uint32_t parity, int b, bool other_issued)
+{
+	mbar_wait(&bar[b], (parity >> b) & 1u);
+	if (other_issued) mbar_wait(&bar[b ^ 1], (parity >> (b ^ 1)) & 1u);
+}
+
 // 2-D, 3-D and 4-D tiled loads of one box into shared memory, completing on `bar` (transaction
 // bytes).
 __device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int c0, int c1, uint64_t *bar)

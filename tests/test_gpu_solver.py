@@ -111,8 +111,8 @@ def test_eval_granular_all_terms(sv, oracle_mod, ref_available, prec):
 
 @pytest.mark.parametrize("prec,tol", [("f64", 1e-6), ("f32", 1e-4)])
 def test_trajectory_film(sv, oracle_mod, ref_available, prec, tol):
-    # the relax/switching film (config-0/1 geometry, reduced to 32x8 cells so the oracle is
-    # quick): dp54, eps 1e-6, <M>/Ms sampled every 1 ps for 0.1 ns
+    # the thin-film relax/switching problem (3.90625 nm x 3.90625 nm x 3 nm cells, reduced to
+    # 32x8 cells so the oracle is quick): dp54, eps 1e-6, <M>/Ms sampled every 1 ps for 0.1 ns
     if not ref_available:
         pytest.skip("reference not built")
     dims, delta = (32, 8, 1), (3.90625e-9, 3.90625e-9, 3e-9)

@@ -85,6 +85,20 @@ def read_peaks():
     return 6650.0, "fallback"
 
 
+def measured_traffic(kernel, dims, precision):
+    """ncu DRAM bytes per launch recorded in profiles/traffic.json for this kernel, grid and
+    precision (None when no capture of that exact case exists)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        entries = json.load(f).get("entries", [])
+    for e in entries:
+        if e["kernel"] == kernel and tuple(e["dims"]) == tuple(dims) and e["precision"] == precision:
+            return e["bytes"]
+    return None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled every 50 ms; the samples whose own
     nvidia-smi timestamp falls in the timed region (widened by one interval on each side) are
@@ -200,6 +214,44 @@ def cpu_rhs_rate(reg, axes, M0, budget_s=10.0):
     return n * evals / el, threads, f"{evals} full RHS evaluations of the {nx}x{ny}x{nz} slab ({el:.1f} s)"
 
 
+def error_vs_fp64(solver, reg, axes, M0):
+    """Relative L2 errors of the solver's H_demag, H_eff and dM/dt at the initial state against the
+    oracle's FP64 evaluation (FFT convolution in double + field loops), the same GPU-computed FP64
+    demag tensor in both (the tensor generator itself is checked against the exact Newell tensor in
+    the tests).  Resets the solver's state to M0."""
+    import ctypes
+
+    import oracle
+    import torch
+    from micromagnum_b200 import _lib
+    nx, ny, nz = DIMS
+    n = nx * ny * nz
+    ex, ey, ez = oracle.padded(nx, ny, nz)
+    T = torch.empty(6 * ex * ey * ez, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().mm_demag_tensor(nx, ny, nz, *DELTA, ex, ey, ez, ctypes.c_void_p(T.data_ptr()),
+                                         ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    Th = T.cpu().numpy()
+    del T
+    c0 = time.perf_counter()
+    orc = oracle.Solver(DIMS, DELTA, np.full(n, 1e6), A=np.full(n, 1.5e-11), alpha=np.full(n, 0.1),
+                        k_uniaxial=np.full(n, 2e5), axis1=axes[reg].T.copy(), P=np.full(n, 0.5), xi=np.full(n, 0.05),
+                        j=(1e12, 0.0, 0.0), terms=("demag", "exchange", "uniaxial", "zhangli"),
+                        tensor=(Th, (ex, ey, ez)), float_norm=False, use_fft=True)
+    orc.M = M0
+    Hr, dMr, Hdr = orc.eval()
+    del orc, Th
+    solver.M = M0
+    H, dM, Hd = (t.cpu().numpy() for t in solver.eval())
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    return {"H_demag": rel(Hd, Hdr), "H_eff": rel(H, Hr), "dMdt": rel(dM, dMr), "measure": "relative L2",
+            "state": "the seeded initial state of the timed run",
+            "reference": "oracle FP64 (FFT convolution in double, field loops), same FP64 tensor",
+            "oracle_s": round(time.perf_counter() - c0, 1)}
+
+
 # ------------------------------------------------------------------------------------------------
 # our arm
 # ------------------------------------------------------------------------------------------------
@@ -276,23 +328,15 @@ def run_ours(args, rank, world, local_rank):
     name, (cnt, tot_ms, tot_bytes) = top
     achieved = (tot_bytes / cnt) / (tot_ms / cnt * 1e-3) / 1e9
     peak, peak_kind = read_peaks()
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get(name)
+    traffic = measured_traffic(name, DIMS, args.precision)
     shares = {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}
-    tfile = {}
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            tfile = json.load(f)
 
     def kernel_roofline(k):
         c, t_ms, b = prof[k]
         a = (b / c) / (t_ms / c * 1e-3) / 1e9
         return {"bound": "hbm", "kernel": k, "achieved": a, "peak": peak, "unit": "GB/s", "frac": a / peak,
-                "peak_kind": peak_kind, "traffic": tfile.get(k), "algorithmic_bytes_per_launch": b / c,
-                "launch_ms": t_ms / c}
+                "peak_kind": peak_kind, "traffic": measured_traffic(k, DIMS, args.precision),
+                "algorithmic_bytes_per_launch": b / c, "launch_ms": t_ms / c}
 
     # ---- end to end through the public API with host buffers -----------------------------------
     h_in = torch.empty(3 * n, dtype=torch.float64, pin_memory=True)
@@ -312,10 +356,11 @@ def run_ours(args, rank, world, local_rank):
     ms_e, att_e, _, _ = timed(e2e_step, args.steps)
     e2e_value = world * n * 6 * att_e / (max_over_ranks(ms_e) * 1e-3)
 
-    cpu = None
+    cpu, err = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, sample = cpu_rhs_rate(reg, axes, M0)
         cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        err = error_vs_fp64(s, reg, axes, M0)
 
     if rank == 0:
         line = {
@@ -333,8 +378,9 @@ def run_ours(args, rank, world, local_rank):
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": tot_bytes / cnt, "launch_ms": tot_ms / cnt,
                          "time_shares": shares},
-            "stage_roofline": kernel_roofline("k_stage") if "k_stage" in prof else None,
+            "stage_roofline": next((kernel_roofline(k) for k in ("k_stage_tma", "k_stage") if k in prof), None),
             "cpu_baseline": cpu,
+            "error_vs_fp64": err,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

@@ -124,11 +124,21 @@ MM_API mm_status mm_scaled_abs_max(int prec, size_t n, const void *M, const void
  * memory: at most 65536 partial maxima of 4096 cells, so n is limited to 268,435,456 cells and
  * larger n returns MM_ERR_INVALID_ARGUMENT.  Nothing in the scratch has to start at zero.  The
  * first call on each device (with that device current) looks up the array's address; make it
- * during set-up, before any stream capture.  Every call on a device uses the same array, so
- * calls that overlap on the device (other streams, other host threads) race: serialise them.
+ * during set-up, before any stream capture.  That address is kept for the life of the process:
+ * a cudaDeviceReset discards the library's device memory and leaves it stale, so a process that
+ * resets a device must not call this entry point on it afterwards.  Every call on a device uses
+ * the same array, so calls that overlap on the device (other streams, other host threads) race:
+ * serialise them.
  * Synchronises `stream`. */
 MM_API mm_status mm_scaled_abs_max_noalloc(int prec, size_t n, const void *M, const void *scale,
                                            double *result_host, void *stream);
+
+/* sqrt(mean over the 3n equations of (|y_error_i| / (eps_rel |y_i| + eps_abs))^2), the scaled
+ * error norm behind rk_adjust_stepsize (evolver/runge_kutta.cpp:98-130 ->
+ * evolver/runge_kutta_cpu.cpp:196-252, Euclidean branch; the reference asserts when CUDA is enabled,
+ * this computes it on the device).  Synchronises `stream`. */
+MM_API mm_status mm_rk_scaled_error_norm(int prec, size_t n, double eps_abs, double eps_rel, const void *y,
+                                         const void *y_error, double *norm_host, void *stream);
 
 /* M_i <- Ms_i M_i / |M_i| (0 where |M_i| == 0).  Replaces VectorMatrix::normalize(Matrix)
  * (matrix/matrix/vector/VectorMatrix.cpp:218-230) as called by the solver after every accepted
@@ -375,6 +385,47 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 MM_API mm_status mm_batch_results(mm_batch *b, mm_batch_result *results_host, void *stream);
 /* Kernel launches in one captured round (with and without k_0 evaluations). */
 MM_API mm_status mm_batch_launches_per_round(mm_batch *b, int *first, int *later);
+
+/* ---- OMF 1.0 vector-field files (rectangular mesh, one segment) ------------------------------
+ * Replace readOMF / writeOMF / OMFHeader (bindings/mmm/io.i; mmm/io/OMFImport.cpp,
+ * OMFExport.cpp, OMFHeader.h) for device fields: requests and results of the served solves and
+ * the reference's own fixture files.  Text, binary-4 and binary-8 data blocks; binary values are
+ * big-endian after the big-endian check value (1234567.0 / 123456789012345.0).  The reference's
+ * writer leaves binary-8 values in host byte order (OMFExport.cpp:171-177), which its own reader
+ * does not read back on a little-endian host; this writer follows the format. */
+typedef enum { MM_OMF_TEXT = 0, MM_OMF_BINARY_4 = 1, MM_OMF_BINARY_8 = 2 } mm_omf_format_t;
+
+typedef struct {
+	char title[256];
+	char desc[4096];               /* the Desc lines, separated by '\n' */
+	char meshunit[64], valueunit[64], meshtype[64];
+	double valuemultiplier;
+	double xmin, ymin, zmin, xmax, ymax, zmax;
+	double ValueRangeMaxMag, ValueRangeMinMag;
+	double xbase, ybase, zbase;
+	double xstepsize, ystepsize, zstepsize;
+	int xnodes, ynodes, znodes;
+	int format;                    /* set by the readers: the data block's mm_omf_format_t */
+} mm_omf_header;
+
+/* Parses an OMF file held in host memory.  M NULL: the header only.  Otherwise M receives the
+ * field (3 * xnodes*ynodes*znodes elements of `prec`, SoA, x fastest) times valuemultiplier, like
+ * readOMF (OMFImport.cpp:294-440).  Synchronises `stream`. */
+MM_API mm_status mm_omf_parse(const void *bytes_host, size_t length, mm_omf_header *header, int prec, void *M,
+                              void *stream);
+/* mm_omf_parse of the file at `path`. */
+MM_API mm_status mm_omf_read(const char *path, mm_omf_header *header, int prec, void *M, void *stream);
+/* Formats the field M (header's xnodes*ynodes*znodes cells) as an OMF file in `format`, with the
+ * reference's header lines, scaling (values divided by max |M| when it exceeds 0.001, unless
+ * MAGNUM_OMF_NOSCALE is set) and 16 significant digits for text (OMFExport.cpp:55-209).  Sets
+ * header->valuemultiplier, ValueRangeMaxMag and ValueRangeMinMag.  *bytes_host is allocated by
+ * the library: release it with mm_omf_free.  Synchronises `stream`. */
+MM_API mm_status mm_omf_format(mm_omf_header *header, int prec, const void *M, int format, char **bytes_host,
+                               size_t *length, void *stream);
+MM_API void mm_omf_free(char *bytes_host);
+/* mm_omf_format written to the file at `path`. */
+MM_API mm_status mm_omf_write(const char *path, mm_omf_header *header, int prec, const void *M, int format,
+                              void *stream);
 
 #ifdef __cplusplus
 }

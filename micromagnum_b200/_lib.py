@@ -87,6 +87,21 @@ class mm_solver_stats(ctypes.Structure):
 
 
 # (name, restype, argtypes) for every entry point of include/mmb200.h
+class mm_omf_header(ctypes.Structure):
+    _fields_ = [
+        ("title", ctypes.c_char * 256), ("desc", ctypes.c_char * 4096), ("meshunit", ctypes.c_char * 64),
+        ("valueunit", ctypes.c_char * 64), ("meshtype", ctypes.c_char * 64), ("valuemultiplier", ctypes.c_double),
+        ("xmin", ctypes.c_double), ("ymin", ctypes.c_double), ("zmin", ctypes.c_double),
+        ("xmax", ctypes.c_double), ("ymax", ctypes.c_double), ("zmax", ctypes.c_double),
+        ("ValueRangeMaxMag", ctypes.c_double), ("ValueRangeMinMag", ctypes.c_double),
+        ("xbase", ctypes.c_double), ("ybase", ctypes.c_double), ("zbase", ctypes.c_double),
+        ("xstepsize", ctypes.c_double), ("ystepsize", ctypes.c_double), ("zstepsize", ctypes.c_double),
+        ("xnodes", ctypes.c_int), ("ynodes", ctypes.c_int), ("znodes", ctypes.c_int), ("format", ctypes.c_int),
+    ]
+
+
+MM_OMF_TEXT, MM_OMF_BINARY_4, MM_OMF_BINARY_8 = 0, 1, 2
+
 _VP, _D, _I, _SZ = ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.c_size_t
 _DP = ctypes.POINTER(ctypes.c_double)
 _PROTOS = [
@@ -104,6 +119,7 @@ _PROTOS = [
     ("mm_fdm_zhangli", _I, [_I, _I, _I, _I, _D, _D, _D, _I, _VP, _VP, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("mm_scaled_abs_max", _I, [_I, _SZ, _VP, _VP, _DP, _VP]),
     ("mm_scaled_abs_max_noalloc", _I, [_I, _SZ, _VP, _VP, _DP, _VP]),
+    ("mm_rk_scaled_error_norm", _I, [_I, _SZ, _D, _D, _VP, _VP, _DP, _VP]),
     ("mm_normalize", _I, [_I, _SZ, _VP, _VP, _VP]),
     ("mm_rk_prepare_step", _I, [_I, _SZ, _I, _D, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
     ("mm_rk_combine_result", _I, [_I, _SZ, _I, _D, _DP, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
@@ -141,6 +157,12 @@ _PROTOS = [
     ("mm_batch_results", _I, [_VP, ctypes.POINTER(mm_batch_result), _VP]),
     ("mm_batch_launches_per_round", _I, [_VP, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("mm_solver_relax", _I, [_VP, _I, _D, _I, ctypes.c_longlong, ctypes.POINTER(ctypes.c_int), _DP, _VP]),
+    ("mm_omf_parse", _I, [_VP, _SZ, ctypes.POINTER(mm_omf_header), _I, _VP, _VP]),
+    ("mm_omf_read", _I, [ctypes.c_char_p, ctypes.POINTER(mm_omf_header), _I, _VP, _VP]),
+    ("mm_omf_format", _I, [ctypes.POINTER(mm_omf_header), _I, _VP, _I, ctypes.POINTER(_VP), ctypes.POINTER(_SZ),
+                           _VP]),
+    ("mm_omf_free", None, [_VP]),
+    ("mm_omf_write", _I, [ctypes.c_char_p, ctypes.POINTER(mm_omf_header), _I, _VP, _I, _VP]),
 ]
 
 EXPORTED = [p[0] for p in _PROTOS]

@@ -1406,8 +1406,9 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	else
 		k_x_fwd<T, false><<<gx, NT, p->smem_x, st>>>(M, reg, ms_tab, S, p->nx, p->ny, p->nz, p->py, p->hx, p->lx,
 		                                             p->rx, (const C *)p->tw_x, p->lp_x);
-	MM_TRY(after_launch("k_x_fwd"));
-	prof_end(tk, "k_x_fwd", 3 * n * s + (reg ? n : 0.0) + half, st);
+	const char *xf_name = staged ? "k_x_fwd_tma" : p->fast_x ? "k_x_fwd_ct" : "k_x_fwd";
+	MM_TRY(after_launch(xf_name));
+	prof_end(tk, xf_name, 3 * n * s + (reg ? n : 0.0) + half, st);
 	if (p->is2d) {
 		const int gy = (p->hx + p->tb_y - 1) / p->tb_y;
 		tk = prof_begin(st);
@@ -1429,8 +1430,9 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		} else
 			k_y<T, false><<<gy, NT, p->smem_y, st>>>(S, p->ny, p->py, p->nz, p->py, p->hx, p->lx, p->ry,
 			                                         (const C *)p->tw_y, p->tb_y);
-		MM_TRY(after_launch("k_y_fwd"));
-		prof_end(tk, "k_y_fwd", half + ypad, st);
+		const char *yf_name = p->tma_y ? "k_y_tma (forward)" : p->fast_y ? "k_y_ct (forward)" : "k_y (forward)";
+		MM_TRY(after_launch(yf_name));
+		prof_end(tk, yf_name, half + ypad, st);
 		dim3 gz((p->hx + p->tb_z - 1) / p->tb_z, p->py, 1);
 		tk = prof_begin(st);
 		if (p->reg_z) {
@@ -1453,8 +1455,9 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		} else
 			k_z_mul<T><<<gz, NT, p->smem_z, st>>>(S, (const T *)p->tensor, p->nz, p->py, p->hx, p->lx, p->qy, p->qz,
 			                                      p->rz, (const C *)p->tw_z, p->tb_z);
-		MM_TRY(after_launch("k_z_mul"));
-		prof_end(tk, "k_z_mul", 2 * ypad + tens, st);
+		const char *z_name = p->reg_z ? "k_z_reg" : p->fast_z ? "k_z_ct" : "k_z_mul";
+		MM_TRY(after_launch(z_name));
+		prof_end(tk, z_name, 2 * ypad + tens, st);
 		tk = prof_begin(st);
 		if (p->tma_y) {
 #define MM_YTI(N) fs_y_tma<T, N, true>(p, st)
@@ -1467,8 +1470,9 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 		} else
 			k_y<T, true><<<gy, NT, p->smem_y, st>>>(S, p->py, p->ny, p->nz, p->py, p->hx, p->lx, p->ry,
 			                                        (const C *)p->tw_y, p->tb_y);
-		MM_TRY(after_launch("k_y_inv"));
-		prof_end(tk, "k_y_inv", half + ypad, st);
+		const char *yi_name = p->tma_y ? "k_y_tma (inverse)" : p->fast_y ? "k_y_ct (inverse)" : "k_y (inverse)";
+		MM_TRY(after_launch(yi_name));
+		prof_end(tk, yi_name, half + ypad, st);
 	}
 	tk = prof_begin(st);
 	if (p->tma_xi) {
@@ -1482,8 +1486,9 @@ mm_status execute(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	} else
 		k_x_inv<T><<<gx, NT, p->smem_x, st>>>(S, H, p->nx, p->ny, p->nz, p->py, p->hx, p->lx, p->rx,
 		                                      (const C *)p->tw_x, p->lp_x);
-	MM_TRY(after_launch("k_x_inv"));
-	prof_end(tk, "k_x_inv", half + 3 * n * s, st);
+	const char *xi_name = p->tma_xi ? "k_x_inv_tma" : p->fast_x ? "k_x_inv_ct" : "k_x_inv";
+	MM_TRY(after_launch(xi_name));
+	prof_end(tk, xi_name, half + 3 * n * s, st);
 	return MM_OK;
 }
 

@@ -1042,6 +1042,7 @@ struct mm_solver {
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 	// staged stage kernel: used when the rows are 16-byte aligned; grid and shared memory per stage
 	bool st_tma = false;
+	int st_resident = 0;             // resident blocks of k_stage on this solver's device
 	int st_grid[MAXS] = {};
 	size_t st_smem[MAXS] = {};
 	StageMaps st_maps{};             // yin set per launch from st_yin
@@ -1200,30 +1201,37 @@ double stage_bytes(const mm_solver *s, const StageCoef &sc)
 	return b;
 }
 
-// Resident blocks of the fused stage kernel on the whole device (occupancy of the S = 6 instance),
-// looked up once; solver creation calls it so that no later call does so during stream capture.
+// The per-thread-load stage kernel needs more than the default 48 KB of dynamic shared memory.
+// The attribute belongs to the current device, so every solver creation sets it on its own device.
 template <typename T, bool COMP, int... S>
-void stage_smem_attrs(std::integer_sequence<int, S...>)
+mm_status stage_smem_attrs(std::integer_sequence<int, S...>)
 {
 	const int bytes = (int)stage_smem<T>();
-	(cudaFuncSetAttribute(k_stage<T, COMP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
+	cudaError_t e = cudaSuccess;
+	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage<T, COMP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                              bytes)
+	                       : e),
+	 ...);
+	MM_CUDA(e);
+	return MM_OK;
 }
 
+// Resident blocks of the fused stage kernel on the current device (occupancy of the S = 6
+// instance).  Solver creation stores the count in the solver, so that no later call queries
+// occupancy during stream capture.
 template <typename T, bool COMP>
-int stage_resident()
+mm_status stage_resident(int *resident)
 {
-	static const int resident = [] {
-		stage_smem_attrs<T, COMP>(std::make_integer_sequence<int, MAXS>());
-		int per_sm = 0;
-		if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<T, COMP, 6>, 256, stage_smem<T>()) !=
-		        cudaSuccess ||
-		    per_sm < 1) {
-			cudaGetLastError();
-			per_sm = stage_min_blocks<T>();
-		}
-		return per_sm * num_sms();
-	}();
-	return resident;
+	MM_TRY((stage_smem_attrs<T, COMP>(std::make_integer_sequence<int, MAXS>())));
+	int per_sm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage<T, COMP, 6>, 256, stage_smem<T>()) !=
+	        cudaSuccess ||
+	    per_sm < 1) {
+		cudaGetLastError();
+		per_sm = stage_min_blocks<T>();
+	}
+	*resident = per_sm * num_sms();
+	return MM_OK;
 }
 
 // Launches the fused stage kernel for stage S on a persistent grid of at most the resident blocks.
@@ -1231,7 +1239,7 @@ template <typename T, bool COMP, int S>
 void stage_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef &sc, const T *yin, const T *yhi,
                   const T *ylo, const KTab<T> *kt, T *yout, DevState *ds, cudaStream_t st)
 {
-	const int resident = stage_resident<T, COMP>();
+	const int resident = s->st_resident;
 	const dim3 tg = stage_grid(s->cfg);
 	const int ntiles = (int)(tg.x * tg.y * tg.z);
 	const int grid = ntiles < resident ? ntiles : resident;
@@ -1420,7 +1428,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		MM_TRY(demag<T>(s, s->m, st));
 		ProfToken tk = prof_begin(st);
 		MM_TRY((launch_stage<T, COMP>(s, a, sc, yhi, yhi, ylo, kt, ys[0], ds, st)));
-		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
+		prof_end(tk, s->st_tma ? "k_stage_tma" : "k_stage", stage_bytes<T>(s, sc), st);
 	} else {
 		const size_t n3 = 3 * s->n;
 		ProfToken tk = prof_begin(st);
@@ -1434,7 +1442,7 @@ mm_status attempt(mm_solver *s, bool eval_k0, cudaStream_t st)
 		MM_TRY(demag<T>(s, yin, st));
 		ProfToken tk = prof_begin(st);
 		MM_TRY((launch_stage<T, COMP>(s, a, sc, yin, yhi, ylo, kt, ys[i & 1], ds, st)));
-		prof_end(tk, "k_stage", stage_bytes<T>(s, sc), st);
+		prof_end(tk, s->st_tma ? "k_stage_tma" : "k_stage", stage_bytes<T>(s, sc), st);
 		if (sc.last) s->last_stage_buf = sc.write_new ? (i & 1) : ((i - 1) & 1);
 	}
 	return MM_OK;
@@ -1668,7 +1676,7 @@ mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uin
 		if (N) cudaFree(N);
 		MM_TRY(r);
 	}
-	stage_resident<T, sizeof(T) == 4>();
+	MM_TRY((stage_resident<T, sizeof(T) == 4>(&s->st_resident)));
 	MM_TRY(stage_tma_setup<T>(s, std::make_integer_sequence<int, MAXS>()));
 	MM_CUDA(cudaStreamSynchronize(st));
 	return MM_OK;
@@ -2275,11 +2283,20 @@ mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 }
 
 template <typename T, bool COMP, int... S>
-void stage_grp_attrs(std::integer_sequence<int, S...>)
+mm_status stage_grp_attrs(std::integer_sequence<int, S...>)
 {
 	const int bytes = (int)stage_smem<T>();
-	(cudaFuncSetAttribute(k_stage_grp<T, COMP, S, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
-	(cudaFuncSetAttribute(k_stage_grp<T, COMP, S, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), ...);
+	cudaError_t e = cudaSuccess;
+	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, false>,
+	                                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+	                       : e),
+	 ...);
+	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, true>,
+	                                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
+	                       : e),
+	 ...);
+	MM_CUDA(e);
+	return MM_OK;
 }
 
 // Captures one round into a graph on the batch's private stream.
@@ -2357,7 +2374,7 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 	b->n_cell3 = (int)c3.size();
 	b->n_cell = (int)c1.size();
 	MM_CUDA(cudaStreamSynchronize(st));
-	stage_grp_attrs<T, sizeof(T) == 4>(std::make_integer_sequence<int, 7>());
+	MM_TRY((stage_grp_attrs<T, sizeof(T) == 4>(std::make_integer_sequence<int, 7>())));
 	MM_TRY(batch_graph<T>(b, 0));
 	MM_TRY(batch_graph<T>(b, 1));
 	return MM_OK;

@@ -294,6 +294,23 @@ __global__ void __launch_bounds__(TPB) k_rk_combine(size_t n3, int nk, double h,
 	}
 }
 
+// ---- scaled error norm of the NR step-size controller (evolver/runge_kutta_cpu.cpp:196-252, the
+// Euclidean branch): sum over all 3N equations of (|err_i| / (eps_rel |y_i| + eps_abs))^2 ------------
+template <typename T>
+__global__ void __launch_bounds__(TPB) k_rk_error_norm2(size_t n3, double eps_abs, double eps_rel,
+                                                        const T *__restrict__ y, const T *__restrict__ yerr,
+                                                        double *out)
+{
+	double acc = 0.0;
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3;
+	     i += (size_t)gridDim.x * blockDim.x) {
+		const double d0 = eps_rel * fabs((double)y[i]) + eps_abs;
+		const double r = fabs((double)yerr[i]) / fabs(d0);
+		acc += r * r;
+	}
+	block_sum_to(out, acc);
+}
+
 template <typename T>
 mm_status finish_energy(double *acc, ScalarScratch *sc, double *energy_host, cudaStream_t st)
 {
@@ -440,6 +457,29 @@ MM_API mm_status mm_scaled_abs_max(int prec, size_t n, const void *M, const void
 	return MM_OK;
 }
 
+MM_API mm_status mm_rk_scaled_error_norm(int prec, size_t n, double eps_abs, double eps_rel, const void *y,
+                                         const void *y_error, double *norm_host, void *stream)
+{
+	if (bad_prec(prec) || n == 0 || !y || !y_error || !norm_host)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_rk_scaled_error_norm: invalid argument");
+	cudaStream_t st = as_stream(stream);
+	ScalarScratch *sc = nullptr;
+	MM_TRY(scalar_scratch(&sc));
+	MM_CUDA(cudaMemsetAsync(sc->dev, 0, sizeof(double), st));
+	const size_t n3 = 3 * n;
+	if (prec == MM_F64)
+		k_rk_error_norm2<double><<<grid_for(n3), TPB, 0, st>>>(n3, eps_abs, eps_rel, (const double *)y,
+		                                                       (const double *)y_error, sc->dev);
+	else
+		k_rk_error_norm2<float><<<grid_for(n3), TPB, 0, st>>>(n3, eps_abs, eps_rel, (const float *)y,
+		                                                      (const float *)y_error, sc->dev);
+	MM_TRY(after_launch("k_rk_error_norm2"));
+	MM_CUDA(cudaMemcpyAsync(sc->host, sc->dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	*norm_host = sqrt(sc->host[0] / (double)n3);
+	return MM_OK;
+}
+
 MM_API mm_status mm_normalize(int prec, size_t n, const void *Ms, void *M, void *stream)
 {
 	if (bad_prec(prec) || n == 0 || !Ms || !M)
@@ -581,7 +621,8 @@ __global__ void __launch_bounds__(NA_FINAL_THREADS) k_scaled_abs_max_final(int b
 	if (threadIdx.x == 0) scratch[NA_MAX_PARTIALS] = best;
 }
 
-// Device address of g_na_scratch on the current device, looked up once per device.
+// Device address of g_na_scratch on the current device, looked up once per device and kept for
+// the life of the process (a cudaDeviceReset of that device would leave it stale).
 mm_status na_scratch(double **out)
 {
 	static std::mutex mu;

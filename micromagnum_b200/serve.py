@@ -119,12 +119,17 @@ class Server:
                             break
                         req = cl.queue[0]
                         res, trans = req.instance.device_bytes(self.precision)
-                        if cl.live and state["used"] + res + trans > self.budget:
+                        # the budget is shared by every class, so an idle class waits too; each
+                        # request fits alone (checked before the run), so memory freed by the
+                        # other classes eventually admits it
+                        if state["used"] + res + trans > self.budget:
                             break
-                        state["used"] += res
+                        state["used"] += res + trans  # set-up scratch held until add() returns
                         stats.peak_resident = max(stats.peak_resident, state["used"])
                         cl.queue.popleft()
                     slot = cl.batch.add(req.instance, req.M0)
+                    with lock:
+                        state["used"] -= trans
                     cl.live[slot] = (req, res, clock() - t0)
                     admitted = True
                 if not cl.live:

@@ -18,6 +18,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import magneto as _magneto
 from ._lib import check, lib
 
 TERMS = {
@@ -29,26 +30,14 @@ TABLEAUS = {"rkf45": _lib.MM_RK_RKF45, "cc45": _lib.MM_RK_CC45, "dp54": _lib.MM_
             "rk23": _lib.MM_RK_RK23}
 
 
-@dataclass
-class RectangularMesh:
-    """magneto/mesh/RectangularMesh.h:7-66 (non-periodic use)."""
-    num_nodes: tuple
-    delta: tuple
-    periodic_bc: tuple = ("", 1)
+class RectangularMesh(_magneto.RectangularMesh):
+    """magnum.mesh.RectangularMesh (src/magnum/mesh/rectangular_mesh.py:22-35): the mesh from
+    the number of cells and the cell size; the solver itself is non-periodic."""
 
-    @property
-    def total_nodes(self) -> int:
-        nx, ny, nz = self.num_nodes
-        return nx * ny * nz
-
-    @property
-    def cell_volume(self) -> float:
-        dx, dy, dz = self.delta
-        return dx * dy * dz
-
-    @property
-    def volume(self) -> float:
-        return self.cell_volume * self.total_nodes
+    def __init__(self, num_nodes, cell_size, periodic_bc: str = "", periodic_repeat=None):
+        nx, ny, nz = (int(v) for v in num_nodes)
+        dx, dy, dz = (float(v) for v in cell_size)
+        super().__init__(nx, ny, nz, dx, dy, dz, periodic_bc, periodic_repeat or -1)
 
 
 @dataclass

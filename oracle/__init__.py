@@ -23,7 +23,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmmref.so")
-REF_SRC = "/root/reference/src/magneto"
+# Root of a MicroMagnum checkout (the directory holding src/magneto), from the environment;
+# only needed to compile _ref/libmmref.so, never at run time.
+REF_ROOT = os.environ.get("MMB200_REFERENCE")
+REF_SRC = os.path.join(REF_ROOT, "src", "magneto") if REF_ROOT else None
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _D = ctypes.c_double
@@ -31,8 +34,10 @@ _D = ctypes.c_double
 
 def build(with_ref: bool = True) -> None:
     """Compile liboracle.so, and _ref/libmmref.so when the reference tree is present."""
-    target = "ref" if (with_ref and os.path.isdir(REF_SRC)) else "all"
-    subprocess.run(["make", "-C", HERE, target], check=True, stdout=subprocess.DEVNULL)
+    if with_ref and REF_SRC and os.path.isdir(REF_SRC):
+        subprocess.run(["make", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True, stdout=subprocess.DEVNULL)
+    else:
+        subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=subprocess.DEVNULL)
 
 
 def _p(a: np.ndarray):
@@ -71,7 +76,7 @@ def reference():
     global _R
     if _R is None:
         if not os.path.exists(REF_SO):
-            if os.path.isdir(REF_SRC):
+            if REF_SRC and os.path.isdir(REF_SRC):
                 build(with_ref=True)
             else:
                 return None

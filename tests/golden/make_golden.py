@@ -6,7 +6,8 @@ Source files (read from the reference tree, which exists only in the build conta
   src/magnum_tests/ref/H1_stray.omf   stray field of M1, PADDING_ROUND_4 (stray_field_test.py:29-50)
   src/magnum_tests/ref/H1_unianiso.omf uniaxial field of M1, axis (1,1,1)/sqrt3, k = 520e3, Ms = 8e5
                                        (anisotropy_test.py:30-47, ref/H1_unianiso.txt)
-Run:  python tests/golden/make_golden.py [/path/to/src/magnum_tests/ref]
+Run:  python tests/golden/make_golden.py /path/to/src/magnum_tests/ref
+      (or set MMB200_REFERENCE to the checkout's root)
 The OMF 'Data Text' section lists one vector per line, x fastest, then y, then z.
 """
 import os
@@ -53,4 +54,9 @@ def main(refdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/magnum_tests/ref")
+    if len(sys.argv) > 1:
+        main(sys.argv[1])
+    elif os.environ.get("MMB200_REFERENCE"):
+        main(os.path.join(os.environ["MMB200_REFERENCE"], "src", "magnum_tests", "ref"))
+    else:
+        sys.exit("usage: make_golden.py <src/magnum_tests/ref> (or set MMB200_REFERENCE)")

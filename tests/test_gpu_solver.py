@@ -109,6 +109,75 @@ def test_eval_granular_all_terms(sv, oracle_mod, ref_available, prec):
     assert rel_l2(dM, dMr) < tol
 
 
+def granular_materials(sv, rng, ngrains):
+    """Region 0 empty (Ms = 0); regions 1..ngrains: grains with their own uniaxial and cubic axes,
+    Zhang-Li current along x."""
+    mats = [sv.Material()]
+    for _ in range(ngrains):
+        a1 = unit_random(rng, 1)[:, 0]
+        a2 = np.cross(a1, unit_random(rng, 1)[:, 0])
+        a2 /= np.linalg.norm(a2)
+        mats.append(sv.Material(Ms=1e6, A=1.5e-11, alpha=0.1, k_uniaxial=2e5, k_cubic=-3e4, axis1=tuple(a1),
+                                axis2=tuple(a2), P=0.5, xi=0.05, j=(1e12, 0.0, 0.0)))
+    return mats
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_staged_kernels_granular_vs_oracle(sv, oracle_mod, ref_available, prec):
+    # the kernels the slab benchmark times: the staged stage kernel k_stage_tma with regions
+    # (nx % 16 == 0) and the TMA-staged x passes whose forward pass scales by the region's Ms
+    # (both x passes take tiles of 2 LPB rows of one plane: ny = 64 is a multiple of that).
+    # 64x64x4 cells, 8 grains (uniaxial + cubic), Zhang-Li j = 1e12 A/m^2, 5% empty cells and an
+    # applied field: H_eff and dM/dt, the first step's increment, then five more steps
+    from micromagnum_b200 import _lib
+    if not ref_available:
+        pytest.skip("reference not built")
+    rng = np.random.default_rng(12)
+    dims, delta = (64, 64, 4), (2e-9, 2e-9, 2e-9)
+    n = int(np.prod(dims))
+    mats = granular_materials(sv, rng, 8)
+    reg = voronoi(dims, 8, rng) + 1
+    reg[rng.random(n) < 0.05] = 0
+    ours, orc = make_pair(sv, oracle_mod, dims, delta, mats, reg,
+                          ("demag", "exchange", "uniaxial", "cubic", "zhangli"), prec, H_ext=(5e3, 0, 1e4),
+                          evolver="dp54", eps_abs=1e-3, eps_rel=1e-4)
+    M0 = unit_random(rng, n) * 1e6
+    ours.M = M0
+    orc.M = M0
+    M0 = orc.M  # zero in the empty cells
+    _lib.profile_reset()
+    _lib.profile_enable(True)
+    try:
+        H, dM, Hd = (t.cpu().numpy() for t in ours.eval())
+        ours.step()
+        torch.cuda.synchronize()
+        ran = set(_lib.profile_read())
+    finally:
+        _lib.profile_enable(False)
+    assert {"k_stage_tma", "k_x_fwd_tma", "k_x_inv_tma"} <= ran, ran
+    Hr, dMr, Hdr = orc.eval()
+    orc.step()
+    tol = 1e-12 if prec == "f64" else 1e-5
+    assert rel_l2(Hd, Hdr) < tol
+    assert rel_l2(H, Hr) < tol
+    assert rel_l2(dM, dMr) < tol
+    # one accepted dp54 step: all seven stages through k_stage_tma; the increment M1 - M0 carries
+    # the stage kernel's arithmetic, the step size the controller's
+    a, b = ours.stats, orc.stats
+    assert a["steps"] == b["steps"] == 1 and a["rejected"] == b["rejected"]
+    assert a["t"] == pytest.approx(b["t"], rel=1e-12)
+    assert a["h_next"] == pytest.approx(b["h_next"], rel=1e-9 if prec == "f64" else 1e-4)
+    assert rel_l2(ours.M.cpu().numpy() - M0, orc.M - M0) < tol
+    for _ in range(5):
+        ours.step()
+        orc.step()
+    a, b = ours.stats, orc.stats
+    assert a["steps"] == b["steps"] and a["rejected"] == b["rejected"]
+    assert a["t"] == pytest.approx(b["t"], rel=1e-10 if prec == "f64" else 1e-4)
+    if prec == "f64":
+        assert rel_l2(ours.M.cpu().numpy(), orc.M) < 1e-12
+
+
 @pytest.mark.parametrize("prec,tol", [("f64", 1e-6), ("f32", 1e-4)])
 def test_trajectory_film(sv, oracle_mod, ref_available, prec, tol):
     # the thin-film relax/switching problem (3.90625 nm x 3.90625 nm x 3 nm cells, reduced to

@@ -255,3 +255,29 @@ def test_conv_methods_agree(oracle_mod, need_ref, dims):
     Hr = oracle_mod.conv(N, dims, pd, M, impl="ref")
     assert rel_l2(Hd, Hr) < 1e-14
     assert rel_l2(Hf, Hd) < 1e-13
+
+
+def test_film_trajectory_fixture_is_the_oracles(oracle_mod, need_ref):
+    # tests/golden/film_trajectories.npz (tests/golden/make_trajectories.py) holds the oracle's
+    # thin-film runs; re-run the first 20 ps of the relaxation and 5 ps of the dynamics and check
+    # the committed samples against them
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    sys.path.insert(0, here)
+    import make_trajectories as film
+    d = np.load(os.path.join(here, "film_trajectories.npz"))
+    s = film.oracle_solver(oracle_mod, 0.5)
+    s.M = film.initial_m() * film.MS
+    t, m = s.solve(2e-11, sample_dt=film.RELAX_DT)
+    assert np.array_equal(t, d["relax_t"][:len(t)])
+    assert np.abs(m / film.MS - d["relax_m"][:len(t)]).max() < 1e-13
+    s = film.oracle_solver(oracle_mod, 0.02, H_ext=tuple(d["dyn_H_ext"]))
+    assert np.allclose(d["dyn_H_ext"], film.applied_field(), rtol=1e-15, atol=0)
+    s.M = d["relax_M"]
+    t, m = s.solve(5e-12, sample_dt=film.DYN_DT)
+    assert np.array_equal(t, d["dyn_t"][:len(t)])
+    assert np.abs(m / film.MS - d["dyn_m"][:len(t)]).max() < 1e-13
+    assert len(d["dyn_t"]) == 1001 and len(d["relax_t"]) == 201
+    for key in ("relax_M", "dyn_M"):
+        assert np.allclose(np.linalg.norm(d[key], axis=0), film.MS, rtol=1e-12)

@@ -124,3 +124,23 @@ def test_request_over_the_budget_is_refused(fake):
     with pytest.raises(MemoryError):
         srv.run(reqs)
     srv.close()
+
+
+def test_budget_is_shared_by_all_size_classes(fake):
+    # requests of three size classes (class bounds 2^17 and 2^20 cells): the device-memory budget
+    # is one pool, so an idle class may not admit past it while the others hold most of it
+    small = make_requests(6, (32, 32, 1), need=lambda i: 12)
+    mid = make_requests(3, (512, 512, 1), need=lambda i: 8)
+    big = make_requests(2, (1024, 1024, 2), need=lambda i: 6)
+    reqs = []
+    for i, r in enumerate(small + mid + big):
+        r.id = i
+        r.arrival = 0.0
+        reqs.append(r)
+    sizes = [sum(r.instance.device_bytes()) for r in reqs]
+    budget = max(sizes) + sizes[0]  # the largest request and one small one at a time, at most
+    srv = serve.Server(memory_budget=budget, rounds_per_tick=2)
+    st = srv.run(reqs)
+    srv.close()
+    assert len(st.completed) == len(reqs) and st.unfinished == 0
+    assert st.peak_resident <= budget

@@ -300,6 +300,14 @@ MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *s
  * with Ms != 0 of |m x H_eff| / Ms (dimensionless torque).  Synchronises `stream`. */
 MM_API mm_status mm_solver_relax_norms(mm_solver *s, double *norms_host3, void *stream);
 
+/* Energies of the current state in J: energies_host5 = {E_stray, E_exch, E_aniso, E_ext, E_tot}
+ * (E_stray = -mu0/2 V sum M.H_stray, stray_field.py:49-52; E_exch = -mu0/2 V sum M.H_exch,
+ * exchange_field.py:57-58; E_aniso = V times the anisotropy functions' return values on the CPU
+ * path, anisotropy_field.py:84-87 with anisotropy_cpu.cpp:29-119; E_ext = -mu0 V sum M.H_ext,
+ * external_field.py:34-35; E_tot their sum, landau_lifshitz_gilbert.py:103-106).  Terms the
+ * solver was not created with contribute 0.  One demag evaluation; synchronises `stream`. */
+MM_API mm_status mm_solver_energies(mm_solver *s, double *energies_host5, void *stream);
+
 enum { MM_RELAX_DEG_PER_NS = 0, MM_RELAX_TORQUE = 1 };
 
 /* Steps (t_max = 1e100, like Solver.solve with a condition that has no time of interest) until

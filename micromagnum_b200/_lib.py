@@ -142,6 +142,7 @@ _PROTOS = [
     ("mm_solver_stats_get", _I, [_VP, ctypes.POINTER(mm_solver_stats), _VP]),
     ("mm_solver_average_M", _I, [_VP, _DP, _VP]),
     ("mm_solver_relax_norms", _I, [_VP, _DP, _VP]),
+    ("mm_solver_energies", _I, [_VP, _DP, _VP]),
     ("mm_batch_instance_bytes", _I, [ctypes.POINTER(mm_batch_instance), _I, ctypes.POINTER(_SZ),
                                      ctypes.POINTER(_SZ)]),
     ("mm_batch_add", _I, [_VP, ctypes.POINTER(mm_batch_instance), _VP, ctypes.POINTER(_I), _VP]),

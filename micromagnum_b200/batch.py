@@ -104,8 +104,17 @@ class Batch:
         check(lib().mm_batch_stop(self._h, int(slot), None))
 
     def set_M(self, index: int, M) -> None:
-        """M of instance `index`, (3, N) or (3N,) in A/m (normalised to Ms in the material)."""
-        v = torch.as_tensor(M, dtype=torch.float64).reshape(-1).cuda().contiguous()
+        """M of instance `index`, (3, N) or (3N,) in A/m (normalised to Ms in the material), or
+        the bytes of an OMF file of the instance's mesh."""
+        if isinstance(M, (bytes, bytearray, memoryview)):
+            from . import omf
+            h, v = omf.parse(bytes(M))
+            if (h.xnodes, h.ynodes, h.znodes) != tuple(self.instances[index].dims):
+                raise ValueError(f"OMF field of {(h.xnodes, h.ynodes, h.znodes)} cells for an instance of "
+                                 f"{tuple(self.instances[index].dims)}")
+            v = v.reshape(-1)
+        else:
+            v = torch.as_tensor(M, dtype=torch.float64).reshape(-1).cuda().contiguous()
         check(lib().mm_batch_set_M(self._h, int(index), ctypes.c_void_p(v.data_ptr()), None))
         torch.cuda.current_stream().synchronize()
 

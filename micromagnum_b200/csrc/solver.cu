@@ -945,6 +945,79 @@ __global__ void __launch_bounds__(256) k_relax_norms(CellArgs<T> a, const T *__r
 	block_max_to(red + 2, tq2);
 }
 
+// Energy sums of the current state, accumulated into acc[0..4]: sum M.H_demag, sum M.H_exch,
+// sum k_u |a x m|^2, sum k_c (s1 s2 + s1 s3 + s2 s3), sum M.H_ext (the reference's E_stray,
+// E_exch, E_aniso and E_ext before their prefactors: stray_field.py:49-52, exchange_field.py:57-58,
+// anisotropy_cpu.cpp:29-119 (the CPU path's energy forms), external_field.py:34-35).  k_u and
+// k_c are recovered from the material record (ku = 2 k_u / (mu0 Ms), kc = -2 k_c / (mu0 Ms)).
+template <typename T>
+__global__ void __launch_bounds__(256) k_energies(CellArgs<T> a, const T *__restrict__ m,
+                                                  const T *__restrict__ Hd, double t, double *acc)
+{
+	__shared__ T msr[256];
+	load_ms_table(a, msr);
+	const int x = blockIdx.x * blockDim.x + threadIdx.x;
+	const int yy = blockIdx.y * blockDim.y + threadIdx.y;
+	const int z = blockIdx.z;
+	double es = 0.0, ex = 0.0, eu = 0.0, ec = 0.0, ez = 0.0;
+	if (x < a.nx && yy < a.ny) {
+		const size_t n = (size_t)a.nx * a.ny * a.nz;
+		const size_t i = ((size_t)z * a.ny + yy) * a.nx + x;
+		const DevMat<T> &M = mat_of(a, i);
+		const double ms = (double)M.Ms;
+		if (ms != 0.0) {
+			const V3<T> mi = load3(m, i, n);
+			const double mx = ms * (double)mi.x, my = ms * (double)mi.y, mz = ms * (double)mi.z;
+			if (a.terms & MM_TERM_DEMAG) {
+				const V3<T> h = load3(Hd, i, n);
+				es = mx * h.x + my * h.y + mz * h.z;
+			}
+			if (a.terms & MM_TERM_EXCHANGE) {
+				const size_t nxy = (size_t)a.nx * a.ny;
+				const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
+				const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
+				const T w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
+				V3<T> sum = v3<T>(0, 0, 0);
+#pragma unroll
+				for (int q = 0; q < 6; ++q) {
+					if (!has[q]) continue;
+					const T nms = a.reg ? msr[a.reg[off[q]]] : M.Ms;
+					if (nms != T(0)) sum = sum + w[q] * (load3(m, off[q], n) - mi);
+				}
+				const V3<T> h = M.cex * sum;
+				ex = mx * h.x + my * h.y + mz * h.z;
+			}
+			if ((a.terms & MM_TERM_UNIAXIAL) && M.ku != T(0)) {
+				const double k = (double)M.ku * MU0 * ms / 2.0;
+				const double ax = M.a1[0], ay = M.a1[1], az = M.a1[2];
+				const double ux = mi.x, uy = mi.y, uz = mi.z;
+				const double cx = ay * uz - az * uy, cy = az * ux - ax * uz, cz = ax * uy - ay * ux;
+				eu = k * (cx * cx + cy * cy + cz * cz);
+			}
+			if ((a.terms & MM_TERM_CUBIC) && M.kc != T(0)) {
+				const double k = -(double)M.kc * MU0 * ms / 2.0;
+				const double ux = mi.x, uy = mi.y, uz = mi.z;
+				const double len = sqrt(ux * ux + uy * uy + uz * uz);
+				const double s = len > 0 ? 1.0 / len : 0.0;
+				const double p1 = s * (M.a1[0] * ux + M.a1[1] * uy + M.a1[2] * uz);
+				const double p2 = s * (M.a2[0] * ux + M.a2[1] * uy + M.a2[2] * uz);
+				const double p3 = s * (M.a3[0] * ux + M.a3[1] * uy + M.a3[2] * uz);
+				const double s1 = p1 * p1, s2 = p2 * p2, s3 = p3 * p3;
+				ec = k * (s1 * s2 + s1 * s3 + s2 * s3);
+			}
+			if (a.terms & MM_TERM_ZEEMAN) {
+				const V3<T> h = zeeman_field(a, t);
+				ez = mx * h.x + my * h.y + mz * h.z;
+			}
+		}
+	}
+	block_sum_to(acc, es);
+	block_sum_to(acc + 1, ex);
+	block_sum_to(acc + 2, eu);
+	block_sum_to(acc + 3, ec);
+	block_sum_to(acc + 4, ez);
+}
+
 // M (A/m, FP64) -> unit state, normalised (LandauLifshitzGilbert.update("M")).
 template <typename T, bool COMP>
 __global__ void k_set_M(size_t n, const double *__restrict__ M, const uint8_t *__restrict__ reg,
@@ -1149,8 +1222,8 @@ mm_status alloc_state(mm_solver *s)
 	MM_CUDA(cudaMemset(s->dst, 0, sizeof(DevState)));
 	MM_CUDA(cudaMallocHost(&s->hst, sizeof(DevState)));
 	std::memset(s->hst, 0, sizeof(DevState));
-	MM_CUDA(cudaMalloc(&s->avg, 4 * sizeof(double)));
-	MM_CUDA(cudaMallocHost(&s->avg_h, 4 * sizeof(double)));
+	MM_CUDA(cudaMalloc(&s->avg, 8 * sizeof(double)));
+	MM_CUDA(cudaMallocHost(&s->avg_h, 8 * sizeof(double)));
 	return MM_OK;
 }
 
@@ -1620,6 +1693,27 @@ mm_status relax_norms(mm_solver *s, double out3[3], cudaStream_t st)
 	return MM_OK;
 }
 
+// Energies of the current state [J]: E_stray, E_exch, E_aniso, E_ext and their sum E_tot (the
+// terms the solver was created with; an absent term contributes 0).  Synchronises.
+template <typename T>
+mm_status energies(mm_solver *s, double out5[5], cudaStream_t st)
+{
+	if (s->cfg.terms & MM_TERM_DEMAG) MM_TRY(demag<T>(s, s->m, st));
+	MM_CUDA(cudaMemsetAsync(s->avg, 0, 5 * sizeof(double), st));
+	k_energies<T><<<cell_grid(s->cfg), dim3(32, 8, 1), 0, st>>>(args_of<T>(s), (const T *)s->m, (const T *)s->hd,
+	                                                            s->t, s->avg);
+	MM_TRY(after_launch("k_energies"));
+	MM_CUDA(cudaMemcpyAsync(s->avg_h, s->avg, 5 * sizeof(double), cudaMemcpyDeviceToHost, st));
+	MM_CUDA(cudaStreamSynchronize(st));
+	const double V = s->cfg.dx * s->cfg.dy * s->cfg.dz;
+	out5[0] = -MU0 / 2.0 * V * s->avg_h[0];
+	out5[1] = -MU0 / 2.0 * V * s->avg_h[1];
+	out5[2] = V * (s->avg_h[2] + s->avg_h[3]);
+	out5[3] = -MU0 * V * s->avg_h[4];
+	out5[4] = out5[0] + out5[1] + out5[2] + out5[3];
+	return MM_OK;
+}
+
 void free_solver(mm_solver *s)
 {
 	if (!s) return;
@@ -1898,6 +1992,13 @@ MM_API mm_status mm_solver_eval(mm_solver *s, double *H_eff, double *dMdt, doubl
 		                                      dMdt, H_demag);
 	}
 	return after_launch("k_eval");
+}
+
+MM_API mm_status mm_solver_energies(mm_solver *s, double *energies_host5, void *stream)
+{
+	if (!s || !energies_host5) return fail(MM_ERR_INVALID_ARGUMENT, "mm_solver_energies: null argument");
+	cudaStream_t st = as_stream(stream);
+	return s->cfg.precision == MM_F64 ? energies<double>(s, energies_host5, st) : energies<float>(s, energies_host5, st);
 }
 
 MM_API mm_status mm_solver_relax_norms(mm_solver *s, double *norms_host3, void *stream)

@@ -20,6 +20,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
+from . import omf
 from .batch import Batch, Instance
 
 
@@ -27,7 +28,7 @@ from .batch import Batch, Instance
 class Request:
     id: int
     instance: Instance
-    M0: np.ndarray
+    M0: object  # (3, N) array in A/m, or the bytes of an OMF file of the instance's mesh
     arrival: float  # seconds after the start of the run
 
 
@@ -40,7 +41,7 @@ class Completed:
     finished: float
     steps: int
     attempts: int
-    M: Optional[np.ndarray] = None
+    M: object = None  # with keep_results: the final M, (3, N) array or (keep_results="omf") OMF bytes
 
     @property
     def latency(self) -> float:
@@ -77,8 +78,10 @@ class _Class:
 class Server:
     def __init__(self, memory_budget: int, precision: str = "f32", eps_abs: float = 1e-3, eps_rel: float = 1e-4,
                  max_torque: float = 1e-4, check_every_nth_step: int = 1, rounds_per_tick: int = 8,
-                 keep_results: bool = False, class_bounds: Sequence[int] = (1 << 17, 1 << 20)):
-        """class_bounds: upper cell counts of the size classes (a last class takes the rest)."""
+                 keep_results=False, class_bounds: Sequence[int] = (1 << 17, 1 << 20)):
+        """class_bounds: upper cell counts of the size classes (a last class takes the rest).
+        keep_results: False, True (final M as a (3, N) array) or "omf" (final M as the bytes of an
+        OMF binary-8 file, the wire format requests may also use for M0)."""
         self.budget = int(memory_budget)
         self.precision = precision
         self.rounds_per_tick = int(rounds_per_tick)
@@ -146,7 +149,12 @@ class Server:
                     r = results[slot]
                     if r["status"] in (1, 2):
                         req, res, adm = cl.live.pop(slot)
-                        M = cl.batch.get_M(slot).cpu().numpy() if self.keep_results else None
+                        M = None
+                        if self.keep_results == "omf":
+                            M = omf.format(cl.batch.get_M(slot), req.instance.dims, req.instance.delta,
+                                           omf.BINARY_8, title=f"request {req.id}")
+                        elif self.keep_results:
+                            M = cl.batch.get_M(slot).cpu().numpy()
                         done.append((Completed(req.id, r["status"], req.arrival, adm, now, r["steps"], r["attempts"],
                                                M), slot, res))
                 for c, slot, res in done:

@@ -204,6 +204,13 @@ class Solver:
         check(lib().mm_solver_relax_norms(self._h, out, _stream_ptr()))
         return tuple(out)
 
+    def energies(self) -> dict:
+        """E_stray, E_exch, E_aniso, E_ext and E_tot [J] at the current state (the reference's
+        state.E_stray ... state.E_tot, landau_lifshitz_gilbert.py:103-106)."""
+        out = (ctypes.c_double * 5)()
+        check(lib().mm_solver_energies(self._h, out, _stream_ptr()))
+        return dict(zip(("E_stray", "E_exch", "E_aniso", "E_ext", "E_tot"), out))
+
     @property
     def deg_per_ns(self) -> float:
         """LandauLifshitzGilbert.calculate_deg_per_ns (landau_lifshitz_gilbert.py:127-131) with the

@@ -23,9 +23,22 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmmref.so")
-# Root of a MicroMagnum checkout (the directory holding src/magneto), from the environment;
-# only needed to compile _ref/libmmref.so, never at run time.
-REF_ROOT = os.environ.get("MMB200_REFERENCE")
+# Root of a MicroMagnum checkout (the directory holding src/magneto and src/magnum): from the
+# environment, else the checkout the last build compiled _ref/libmmref.so from (recorded in
+# _ref/checkout by build()).  Only needed to compile _ref/libmmref.so and by the tests that run the
+# reference's Python package; absent on machines without a checkout.
+REF_RECORD = os.path.join(HERE, "_ref", "checkout")
+
+
+def _checkout():
+    root = os.environ.get("MMB200_REFERENCE")
+    if not root and os.path.exists(REF_RECORD):
+        with open(REF_RECORD) as f:
+            root = f.read().strip()
+    return root if root and os.path.isdir(os.path.join(root, "src")) else None
+
+
+REF_ROOT = _checkout()
 REF_SRC = os.path.join(REF_ROOT, "src", "magneto") if REF_ROOT else None
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -36,6 +49,8 @@ def build(with_ref: bool = True) -> None:
     """Compile liboracle.so, and _ref/libmmref.so when the reference tree is present."""
     if with_ref and REF_SRC and os.path.isdir(REF_SRC):
         subprocess.run(["make", "-C", HERE, "ref", f"REF={REF_SRC}"], check=True, stdout=subprocess.DEVNULL)
+        with open(REF_RECORD, "w") as f:
+            f.write(REF_ROOT + "\n")
     else:
         subprocess.run(["make", "-C", HERE, "all"], check=True, stdout=subprocess.DEVNULL)
 
@@ -82,7 +97,7 @@ def reference():
                 return None
         _R = ctypes.CDLL(REF_SO)
         for name in ("mmref_exchange", "mmref_uniaxial_anisotropy", "mmref_cubic_anisotropy",
-                     "mmref_scaled_abs_max"):
+                     "mmref_scaled_abs_max", "mmref_rk_adjust_stepsize"):
             getattr(_R, name).restype = _D
         _R.mmref_round_tensor_dimension.restype = ctypes.c_int
     return _R

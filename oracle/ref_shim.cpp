@@ -22,8 +22,10 @@
 #include "mmm/demag/tensor_round.h"
 #include "math/conv/SymmetricMatrixVectorConvolution_Simple.h"
 #include "math/ScaledAbsMax.h"
+#include "evolver/runge_kutta.h"
 
 #include <cstring>
+#include <vector>
 #include <string>
 
 // ---- stand-ins for src/magneto/Magneto.cpp (CPU mode, no profiling, logging dropped) ----
@@ -71,6 +73,18 @@ void copy_out(const VectorMatrix &v, double *dst)
 	std::memcpy(dst, acc.ptr_x(), sizeof(double) * n);
 	std::memcpy(dst + n, acc.ptr_y(), sizeof(double) * n);
 	std::memcpy(dst + 2 * n, acc.ptr_z(), sizeof(double) * n);
+}
+
+ButcherTableau tableau(int s, const double *a, const double *b, const double *c, const double *ec)
+{
+	ButcherTableau tab(s);
+	for (int i = 0; i < s; ++i) {
+		tab.setA(i, a[i]);
+		tab.setC(i, c[i]);
+		tab.setEC(i, ec[i]);
+		for (int j = 0; j < s; ++j) tab.setB(i, j, b[i * s + j]);
+	}
+	return tab;
 }
 
 } // namespace
@@ -199,6 +213,45 @@ void mmref_normalize(int nx, int ny, int nz, const double *Ms, double *M)
 	Matrix s = scalar_field(nx, ny, nz, Ms);
 	m.normalize(s);
 	copy_out(m, M);
+}
+
+// src/magneto/evolver/runge_kutta.cpp:32-48 rk_prepare_step (CPU path: runge_kutta_cpu.cpp).
+// tab: s stages, b row-major s x s; k: six arrays (unused ones may repeat k[0], as the caller
+// magnum/evolver/runge_kutta.py:113 passes them).
+void mmref_rk_prepare_step(int nx, int ny, int nz, int step, double h, int s, const double *a, const double *b,
+                           const double *c, const double *ec, const double *const *k, const double *y, double *ytmp)
+{
+	ensure_matty();
+	ButcherTableau tab = tableau(s, a, b, c, ec);
+	std::vector<VectorMatrix> kv;
+	for (int i = 0; i < 6; ++i) kv.push_back(vector_field(nx, ny, nz, k[i]));
+	VectorMatrix yv = vector_field(nx, ny, nz, y), yt(Shape(nx, ny, nz));
+	rk_prepare_step(step, h, tab, kv[0], kv[1], kv[2], kv[3], kv[4], kv[5], yv, yt);
+	copy_out(yt, ytmp);
+}
+
+// src/magneto/evolver/runge_kutta.cpp:68-96 rk_combine_result, the six-vector form (the only one
+// the SWIG module binds, bindings/evolver.i:79-95).
+void mmref_rk_combine_result(int nx, int ny, int nz, double h, int s, const double *a, const double *b,
+                             const double *c, const double *ec, const double *const *k, double *y, double *y_error)
+{
+	ensure_matty();
+	ButcherTableau tab = tableau(s, a, b, c, ec);
+	std::vector<VectorMatrix> kv;
+	for (int i = 0; i < 6; ++i) kv.push_back(vector_field(nx, ny, nz, k[i]));
+	VectorMatrix yv = vector_field(nx, ny, nz, y), ye(Shape(nx, ny, nz));
+	rk_combine_result(h, tab, kv[0], kv[1], kv[2], kv[3], kv[4], kv[5], yv, ye);
+	copy_out(yv, y);
+	copy_out(ye, y_error);
+}
+
+// src/magneto/evolver/runge_kutta.cpp:98-130 rk_adjust_stepsize (the NR controller's rule).
+double mmref_rk_adjust_stepsize(int nx, int ny, int nz, int order, double h, double eps_abs, double eps_rel,
+                                const double *y, const double *y_error)
+{
+	ensure_matty();
+	VectorMatrix yv = vector_field(nx, ny, nz, y), ye = vector_field(nx, ny, nz, y_error);
+	return rk_adjust_stepsize(order, h, eps_abs, eps_rel, yv, ye);
 }
 
 } // extern "C"

@@ -161,9 +161,10 @@ def test_nr_step_size_rule():
 def magnum_pkg(monkeypatch):
     """The unchanged MicroMagnum package (src/magnum of the checkout named by MMB200_REFERENCE),
     imported with this module installed as its native backend the way INTEGRATION.md binds it."""
-    root = os.environ.get("MMB200_REFERENCE")
+    import oracle
+    root = oracle.REF_ROOT
     if not root or not os.path.isdir(os.path.join(root, "src", "magnum")):
-        pytest.skip("MMB200_REFERENCE does not name a MicroMagnum checkout")
+        pytest.skip("no MicroMagnum checkout (MMB200_REFERENCE, or the one the build compiled)")
     for name in [k for k in sys.modules if k == "magnum" or k.startswith("magnum.")]:
         monkeypatch.delitem(sys.modules, name)
     monkeypatch.setitem(sys.modules, "magnum.magneto_cuda", mg)

@@ -78,3 +78,34 @@ def test_admission_waits_for_memory(mods):
     srv.close()
     assert len(stats.completed) == len(reqs)
     assert stats.peak_resident <= budget
+
+
+def test_omf_wire_format(mods):
+    # requests whose M0 is an OMF file (text for some, binary 8 for others) and results returned as
+    # OMF binary-8 files give the same solves as the array path, bit for bit
+    from micromagnum_b200 import omf
+    batch, serve = mods
+    rng = np.random.default_rng(23)
+    reqs = requests(batch, serve, rng, 4, rate=500.0)
+    import torch
+    wire = []
+    for r in reqs:
+        fmt = omf.TEXT if r.id % 2 else omf.BINARY_8
+        data = omf.format(torch.as_tensor(r.M0).cuda(), r.instance.dims, r.instance.delta, fmt)
+        # with MAGNUM_OMF_NOSCALE unset the writer divides by max |M|; the round trip is exact for
+        # binary 8 only up to the multiplier's 16 digits, so both paths start from the parsed field
+        r.M0 = omf.parse(data)[1].cpu().numpy()
+        wire.append(serve.Request(r.id, r.instance, data, r.arrival))
+    kw = dict(memory_budget=8 << 30, max_torque=5e-2, check_every_nth_step=5, rounds_per_tick=4)
+    srv = serve.Server(keep_results=True, **kw)
+    plain = {c.id: c for c in srv.run(reqs).completed}
+    srv.close()
+    srv = serve.Server(keep_results="omf", **kw)
+    got = {c.id: c for c in srv.run(wire).completed}
+    srv.close()
+    assert set(got) == set(plain) == {r.id for r in reqs}
+    for r in reqs:
+        h, M = omf.parse(got[r.id].M)
+        assert (h.xnodes, h.ynodes, h.znodes) == tuple(r.instance.dims) and h.title == f"request {r.id}".encode()
+        assert got[r.id].steps == plain[r.id].steps
+        assert np.abs(M.cpu().numpy() - plain[r.id].M).max() <= 1e-15 * r.instance.Ms

@@ -306,3 +306,42 @@ def test_torque_relaxation_criterion(sv, oracle_mod):
                             float_norm=False)
     orc.M = s.M.cpu().numpy()
     assert orc.relax_norms()[2] == pytest.approx(s.last_relax_value, rel=1e-9)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_energies_vs_oracle(sv, oracle_mod, ref_available, prec):
+    # E_stray, E_exch, E_aniso (uniaxial + cubic), E_ext and E_tot of a granular box with empty
+    # cells against the oracle's fields and energy-returning term functions
+    if not ref_available:
+        pytest.skip("reference not built")
+    rng = np.random.default_rng(21)
+    dims, delta = (24, 20, 4), (2e-9, 2e-9, 3e-9)
+    n = int(np.prod(dims))
+    mats = granular_materials(sv, rng, 6)
+    reg = voronoi(dims, 6, rng) + 1
+    reg[rng.random(n) < 0.05] = 0
+    Hx = (5e3, -2e3, 1e4)
+    ours, orc = make_pair(sv, oracle_mod, dims, delta, mats, reg,
+                          ("demag", "exchange", "uniaxial", "cubic", "zhangli"), prec, H_ext=Hx)
+    M = unit_random(rng, n) * 1e6
+    ours.M = M
+    orc.M = M
+    M = orc.M  # zero in the empty cells
+    e = ours.energies()
+    _, _, Hd = orc.eval()
+    V = float(np.prod(delta))
+    Ms = np.array([mats[r].Ms for r in reg])
+    A = np.array([mats[r].A for r in reg])
+    ku = np.array([mats[r].k_uniaxial for r in reg])
+    kc = np.array([mats[r].k_cubic for r in reg])
+    a1 = np.array([mats[r].axis1 for r in reg]).T.copy()
+    a2 = np.array([mats[r].axis2 for r in reg]).T.copy()
+    ref = {"E_stray": -MU0 / 2 * V * float((M * Hd).sum()),
+           "E_exch": oracle_mod.exchange(*dims, *delta, Ms, A, M)[1],
+           "E_aniso": V * (oracle_mod.uniaxial_anisotropy(a1, ku, Ms, M)[1]
+                           + oracle_mod.cubic_anisotropy(a1, a2, kc, Ms, M)[1]),
+           "E_ext": -MU0 * V * float((M * np.array(Hx).reshape(3, 1)).sum())}
+    ref["E_tot"] = sum(ref.values())
+    tol = 1e-12 if prec == "f64" else 1e-5
+    for k, v in ref.items():
+        assert e[k] == pytest.approx(v, rel=tol), (k, e[k], v)

@@ -175,7 +175,9 @@ def test_staged_kernels_granular_vs_oracle(sv, oracle_mod, ref_available, prec):
     assert a["steps"] == b["steps"] and a["rejected"] == b["rejected"]
     assert a["t"] == pytest.approx(b["t"], rel=1e-10 if prec == "f64" else 1e-4)
     if prec == "f64":
-        assert rel_l2(ours.M.cpu().numpy(), orc.M) < 1e-12
+        # rounding differences of the single evaluations (~1e-16) accumulate through the step-size
+        # feedback over the steps, as in the other multi-step comparisons
+        assert rel_l2(ours.M.cpu().numpy(), orc.M) < 1e-10
 
 
 @pytest.mark.parametrize("prec,tol", [("f64", 1e-6), ("f32", 1e-4)])

@@ -169,11 +169,20 @@ MM_API int mm_round_tensor_dimension(int dim, int periodic, int padding);
  * N_out (device, 6*ex*ey*ez doubles, component index fastest then x, y, z: the reference's
  * Matrix(Shape(6, ex, ey, ez)) layout, mmm/demag/tensor.cpp:41,167-180).  ex/ey/ez are the
  * padded sizes (mm_round_tensor_dimension).  Replaces magneto.GenerateDemagTensor
- * (bindings/mmm/demag.i:27-42 -> mmm/demag/demag_tensor.cpp:116-186).  Periodic boundaries
- * return MM_ERR_UNSUPPORTED; a tensor computed elsewhere can still be passed to
- * mm_conv_create. */
+ * (bindings/mmm/demag.i:27-42 -> mmm/demag/demag_tensor.cpp:116-186) for non-periodic meshes
+ * (padded sizes below 2n - 1 return MM_ERR_UNSUPPORTED; mm_demag_tensor_periodic takes them). */
 MM_API mm_status mm_demag_tensor(int nx, int ny, int nz, double dx, double dy, double dz,
                                  int ex, int ey, int ez, double *N_out, void *stream);
+
+/* The demag tensor with periodic boundaries along the axes whose pbc_* is set (e == n there,
+ * e >= 2n - 1 elsewhere; round_tensor_dimension), `repeat` periodic images per periodic axis and
+ * the sum of the images beyond them (the reference's infinity correction, switched off like the
+ * reference's by the environment variable MAGNUM_DEMAG_NO_INFINITY_CORRECTION).  Replaces
+ * GenerateDemagTensor / calculateDemagTensor for periodic meshes (mmm/demag/demag_tensor.cpp:116-186,
+ * mmm/demag/tensor.cpp:35-191).  Without periodic axes it is mm_demag_tensor.  Stream-ordered. */
+MM_API mm_status mm_demag_tensor_periodic(int nx, int ny, int nz, double dx, double dy, double dz, int pbc_x,
+                                          int pbc_y, int pbc_z, int repeat, int ex, int ey, int ez, double *N_out,
+                                          void *stream);
 
 /* Zero-padded FFT convolution H = N * M with a symmetric tensor field.  Replaces
  * magneto.SymmetricMatrixVectorConvolution_FFT (bindings/math.i:27-33 ->
@@ -237,6 +246,13 @@ typedef struct {
 	 * rejected attempt's last stage as its first (runge_kutta.py:67-70,99-100,131-134).
 	 * 0: re-evaluate the first stage after a rejection. */
 	int fsal_reuse_after_reject;
+	/* Periodic boundaries (the mesh's periodic_bc, RectangularMesh.h:23-26): pbc[a] != 0 makes
+	 * axis a periodic for the exchange stencil and the demag tensor (no zero padding along it);
+	 * pbc_repeat is the number of periodic images, <= 0 for the reference's defaults 15, 3, 2 for
+	 * one, two, three periodic axes (RectangularMesh.h:10-19).  The Zhang-Li gradient stays
+	 * one-sided at the box faces, as in the reference (fdm_zhangli_cpu.cpp:100-200). */
+	int pbc[3];
+	int pbc_repeat;
 } mm_solver_config;
 
 typedef struct {

@@ -50,6 +50,7 @@ class mm_solver_config(ctypes.Structure):
         ("eps_abs", ctypes.c_double), ("eps_rel", ctypes.c_double), ("h0", ctypes.c_double),
         ("H_ext", ctypes.c_double * 3), ("H_pulse", ctypes.c_double * 3),
         ("pulse_rise", ctypes.c_double), ("fsal_reuse_after_reject", ctypes.c_int),
+        ("pbc", ctypes.c_int * 3), ("pbc_repeat", ctypes.c_int),
     ]
 
 
@@ -125,6 +126,7 @@ _PROTOS = [
     ("mm_rk_combine_result", _I, [_I, _SZ, _I, _D, _DP, _DP, ctypes.POINTER(_VP), _VP, _VP, _VP]),
     ("mm_round_tensor_dimension", _I, [_I, _I, _I]),
     ("mm_demag_tensor", _I, [_I, _I, _I, _D, _D, _D, _I, _I, _I, _VP, _VP]),
+    ("mm_demag_tensor_periodic", _I, [_I, _I, _I, _D, _D, _D, _I, _I, _I, _I, _I, _I, _I, _VP, _VP]),
     ("mm_conv_create", _I, [ctypes.POINTER(_VP), _I, _I, _I, _I, _I, _I, _I, _VP, _VP]),
     ("mm_conv_execute", _I, [_VP, _VP, _VP, _VP]),
     ("mm_conv_destroy", _I, [_VP]),

@@ -1237,9 +1237,11 @@ template <typename T>
 mm_status fs_setup(ConvPlan *p)
 {
 	MM_TRY(fft_reg_init());
-	p->fast_x = fs_len_ok<T>(p->px);
-	p->fast_y = !p->is2d && fs_len_ok<T>(p->py);
-	p->fast_z = !p->is2d && p->pz >= 2 && p->pz <= 64 && (p->pz & (p->pz - 1)) == 0;
+	// the power-of-two passes skip the zero upper half of a forward transform, so an axis without
+	// zero padding (a periodic one, padded length n) takes the generic mixed-radix passes
+	p->fast_x = fs_len_ok<T>(p->px) && 2 * p->nx <= p->px;
+	p->fast_y = !p->is2d && fs_len_ok<T>(p->py) && 2 * p->ny <= p->py;
+	p->fast_z = !p->is2d && p->pz >= 2 && p->pz <= 64 && (p->pz & (p->pz - 1)) == 0 && 2 * p->nz <= p->pz;
 	mm_status r = MM_OK;
 #define MM_SETUP(N) r = fs_setup_len<T, N>()
 	if (p->fast_x) { MM_FS_SWITCH(p->px, MM_SETUP); MM_TRY(r); }

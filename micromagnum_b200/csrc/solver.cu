@@ -152,6 +152,7 @@ struct CellArgs {
 	T idx2, idy2, idz2;            // 1/(2 dx) ... (Zhang-Li central differences)
 	T idx1, idy1, idz1;            // 1/dx ...     (one-sided differences)
 	int terms;
+	int pbc;                       // periodic axes: bit 0 x, bit 1 y, bit 2 z (exchange stencil)
 	const uint8_t *reg;            // nullptr: every cell is region 0
 	const DevMat<T> *mat;
 	int nmat;
@@ -235,6 +236,28 @@ __device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> 
 	}
 }
 
+// The six neighbours x-1, x+1, y-1, y+1, z-1, z+1 of cell i = (x, yy, z): whether each exists and
+// its index.  Along a periodic axis the face cells wrap around (exchange_cpu.cpp:141-235).
+template <typename T>
+__device__ __forceinline__ void neighbours(const CellArgs<T> &a, int x, int yy, int z, size_t i, bool (&has)[6],
+                                           size_t (&off)[6])
+{
+	const size_t nx = a.nx, nxy = (size_t)a.nx * a.ny, wy = (size_t)(a.ny - 1) * nx, wz = (size_t)(a.nz - 1) * nxy;
+	const bool px = a.pbc & 1, py = a.pbc & 2, pz = a.pbc & 4;
+	has[0] = x > 0 || px;
+	off[0] = x > 0 ? i - 1 : i + (nx - 1);
+	has[1] = x < a.nx - 1 || px;
+	off[1] = x < a.nx - 1 ? i + 1 : i - (nx - 1);
+	has[2] = yy > 0 || py;
+	off[2] = yy > 0 ? i - nx : i + wy;
+	has[3] = yy < a.ny - 1 || py;
+	off[3] = yy < a.ny - 1 ? i + nx : i - wy;
+	has[4] = z > 0 || pz;
+	off[4] = z > 0 ? i - nxy : i + wz;
+	has[5] = z < a.nz - 1 || pz;
+	off[5] = z < a.nz - 1 ? i + nxy : i - wz;
+}
+
 // Effective field (without the demag term) and dm/dt of one cell of the unit-m field y.
 // Hd: demag field of the cell (added when the term is on); msr: Ms per region (shared memory).
 // The six neighbours are loaded once and serve both the exchange stencil and the Zhang-Li
@@ -255,9 +278,9 @@ __device__ __forceinline__ bool cell_rhs(const CellArgs<T> &a, const T *__restri
 		return false;
 	}
 	const V3<T> m = load3(y, i, n);
-	const size_t nxy = (size_t)a.nx * a.ny;
-	const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
-	const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
+	bool has[6];
+	size_t off[6];
+	neighbours(a, x, yy, z, i, has, off);
 	V3<T> nb[6];
 	T nms[6];
 #pragma unroll
@@ -973,9 +996,9 @@ __global__ void __launch_bounds__(256) k_energies(CellArgs<T> a, const T *__rest
 				es = mx * h.x + my * h.y + mz * h.z;
 			}
 			if (a.terms & MM_TERM_EXCHANGE) {
-				const size_t nxy = (size_t)a.nx * a.ny;
-				const bool has[6] = {x > 0, x < a.nx - 1, yy > 0, yy < a.ny - 1, z > 0, z < a.nz - 1};
-				const size_t off[6] = {i - 1, i + 1, i - a.nx, i + a.nx, i - nxy, i + nxy};
+				bool has[6];
+				size_t off[6];
+				neighbours(a, x, yy, z, i, has, off);
 				const T w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
 				V3<T> sum = v3<T>(0, 0, 0);
 #pragma unroll
@@ -1141,6 +1164,7 @@ void fill_args(mm_solver *s, CellArgs<T> &a)
 	a.idx1 = (T)(1.0 / c.dx); a.idy1 = (T)(1.0 / c.dy); a.idz1 = (T)(1.0 / c.dz);
 	a.idx2 = (T)(1.0 / (2 * c.dx)); a.idy2 = (T)(1.0 / (2 * c.dy)); a.idz2 = (T)(1.0 / (2 * c.dz));
 	a.terms = c.terms;
+	a.pbc = (c.pbc[0] ? 1 : 0) | (c.pbc[1] ? 2 : 0) | (c.pbc[2] ? 4 : 0);
 	a.reg = s->reg;
 	a.mat = (const DevMat<T> *)s->mat;
 	a.nmat = s->nmat;
@@ -1410,7 +1434,9 @@ mm_status stage_tma_setup(mm_solver *s, std::integer_sequence<int, S...>)
 {
 	constexpr bool COMP = sizeof(T) == 4;
 	const char *env = std::getenv("MMB200_STAGE_TMA");
-	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr) && !(env && env[0] == '0');
+	// the staged kernel's halo boxes do not wrap around: periodic meshes take the per-thread kernel
+	const bool periodic = s->cfg.pbc[0] || s->cfg.pbc[1] || s->cfg.pbc[2];
+	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr) && !(env && env[0] == '0') && !periodic;
 	if (!s->st_tma) return MM_OK;
 	mm_status r = stage_tma_maps<T>(s);
 	((r = (r == MM_OK && S < s->tab.s) ? stage_tma_prepare<T, COMP, S>(s) : r), ...);
@@ -1762,7 +1788,11 @@ mm_status create_impl(mm_solver *s, int nmat, const mm_material *mats, const uin
 		const size_t tb = sizeof(double) * 6 * (size_t)s->px * s->py * s->pz;
 		if (!tensor) {
 			MM_CUDA(cudaMalloc(&N, tb));
-			const mm_status r = mm_demag_tensor(c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, s->px, s->py, s->pz, N, st);
+			const int naxes = (c.pbc[0] != 0) + (c.pbc[1] != 0) + (c.pbc[2] != 0);
+			const int repeat = c.pbc_repeat > 0 ? c.pbc_repeat : (naxes == 1 ? 15 : naxes == 2 ? 3 : 2);
+			const mm_status r = mm_demag_tensor_periodic(c.nx, c.ny, c.nz, c.dx, c.dy, c.dz, c.pbc[0] != 0,
+			                                             c.pbc[1] != 0, c.pbc[2] != 0, repeat, s->px, s->py,
+			                                             s->pz, N, st);
 			if (r != MM_OK) { cudaFree(N); return r; }
 		}
 		const mm_status r = conv_plan_create(&s->conv, c.precision, c.nx, c.ny, c.nz, s->px, s->py, s->pz,
@@ -1824,9 +1854,9 @@ mm_status solver_create(mm_solver **out, const mm_solver_config *config, int num
 	s->cfg = c;
 	s->n = (size_t)c.nx * c.ny * c.nz;
 	s->tab = make_tableau(c.tableau);
-	s->px = mm_round_tensor_dimension(c.nx, 0, c.padding);
-	s->py = mm_round_tensor_dimension(c.ny, 0, c.padding);
-	s->pz = mm_round_tensor_dimension(c.nz, 0, c.padding);
+	s->px = mm_round_tensor_dimension(c.nx, c.pbc[0] != 0, c.padding);
+	s->py = mm_round_tensor_dimension(c.ny, c.pbc[1] != 0, c.padding);
+	s->pz = mm_round_tensor_dimension(c.nz, c.pbc[2] != 0, c.padding);
 	if (s->pz > 0 && s->pz < min_pz) s->pz = min_pz;
 	if (s->px <= 0 || s->py <= 0 || s->pz <= 0) {
 		delete s;

@@ -22,6 +22,8 @@
 #include "mm_common.cuh"
 
 #include <cmath>
+#include <cstdlib>
+#include <mutex>
 #include <vector>
 
 namespace mm {
@@ -69,11 +71,17 @@ void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w)
 	}
 }
 
+// The node/weight table lives in device memory, so each device gets its own (built on first use).
 mm_status gl_table(GLTable **out)
 {
-	static GLTable tab;
-	static bool ready = false;
-	if (!ready) {
+	static std::mutex mu;
+	static std::vector<GLTable> tabs;
+	int dev = 0;
+	MM_CUDA(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lock(mu);
+	if ((int)tabs.size() <= dev) tabs.resize(dev + 1);
+	GLTable &tab = tabs[dev];
+	if (!tab.x) {
 		std::vector<double> hx, hw, x, w;
 		for (int n = 1; n <= GL_MAX; ++n) {
 			if (n == 1) { x = {0.0}; w = {2.0}; }
@@ -85,7 +93,6 @@ mm_status gl_table(GLTable **out)
 		MM_CUDA(cudaMalloc(&tab.w, hw.size() * sizeof(double)));
 		MM_CUDA(cudaMemcpy(tab.x, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice));
 		MM_CUDA(cudaMemcpy(tab.w, hw.data(), hw.size() * sizeof(double), cudaMemcpyHostToDevice));
-		ready = true;
 	}
 	*out = &tab;
 	return MM_OK;
@@ -249,6 +256,231 @@ __global__ void __launch_bounds__(128) k_demag_tensor(int nx, int ny, int nz, do
 	}
 }
 
+// ---- periodic boundaries (tensor.cpp:35-165 with demag_tensor.cpp:116-186) --------------------
+// Along a periodic axis the tensor of offset i sums the images i + r n (r < R, the repetitions);
+// the octant scatter adds the mirrored images -(i + r n), so an entry sums displacements from
+// -R n to (R - 1) n around it.  Offsets that coincide with their mirror (i + r n == 0) count
+// half on each side, as the reference divides by its "mcs" factor.  The images beyond the R-th
+// (the reference's infinity correction, tensor.cpp:60-165) are far from the box: their sum is the
+// point-dipole tensor (V / 4 pi) d_a d_b (1 / r), here summed explicitly over TAIL_M further images
+// and integrated in closed form beyond (line integrals with the first Euler-Maclaurin correction for
+// the images along one periodic axis, quadrant integrals for the far corner of two periodic axes,
+// tensor.cpp:104-161), below 1e-9 of the tail sums.  The reference approximates the same sums
+// by asymptotic expansions; no three-axis corner term exists there, nor here.
+constexpr int TAIL_M = 32;
+
+// (V / 4 pi) d_a d_b (1 / r) at r = P: the far-field negated tensor of one cell (xx xy xz yy yz zz)
+__device__ void point_dipole(const double P[3], double V4, double *v)
+{
+	const double r2 = P[0] * P[0] + P[1] * P[1] + P[2] * P[2];
+	const double ir = rsqrt(r2), ir3 = ir * ir * ir, ir5 = ir3 * ir * ir;
+	v[0] += V4 * (3 * P[0] * P[0] * ir5 - ir3);
+	v[1] += V4 * 3 * P[0] * P[1] * ir5;
+	v[2] += V4 * 3 * P[0] * P[2] * ir5;
+	v[3] += V4 * (3 * P[1] * P[1] * ir5 - ir3);
+	v[4] += V4 * 3 * P[1] * P[2] * ir5;
+	v[5] += V4 * (3 * P[2] * P[2] * ir5 - ir3);
+}
+
+__device__ __forceinline__ int sym_idx(int a, int b)
+{
+	const int lo = a < b ? a : b, hi = a < b ? b : a;
+	return lo == 0 ? hi : (lo == 1 ? 2 + hi : 5);
+}
+
+// Integral over s in [0, inf) of d_a d_b (1 / r) at r = P + s e_A (P_A > 0), added times f.
+__device__ void line_integral(const double P[3], int A, double f, double *v)
+{
+	const int B = (A + 1) % 3, C = (A + 2) % 3;
+	const double x0 = P[A], y = P[B], z = P[C];
+	const double r0 = sqrt(x0 * x0 + y * y + z * z), w = x0 + r0, ir3 = 1.0 / (r0 * r0 * r0);
+	const double q = (w + r0) * ir3 / (w * w);
+	v[sym_idx(A, A)] += f * x0 * ir3;
+	v[sym_idx(A, B)] += f * y * ir3;
+	v[sym_idx(A, C)] += f * z * ir3;
+	v[sym_idx(B, B)] += f * (y * y * q - 1.0 / (r0 * w));
+	v[sym_idx(B, C)] += f * y * z * q;
+	v[sym_idx(C, C)] += f * (z * z * q - 1.0 / (r0 * w));
+}
+
+// Integral over s, t in [0, inf) of d_a d_b (1 / r) at r = P + s e_A + t e_B (P_A, P_B > 0).
+__device__ void quadrant_integral(const double P[3], int A, int B, double f, double *v)
+{
+	const int C = 3 - A - B;
+	const double x0 = P[A], y0 = P[B], z = P[C];
+	const double r0 = sqrt(x0 * x0 + y0 * y0 + z * z);
+	const double a2 = x0 * x0 + z * z, b2 = y0 * y0 + z * z;
+	const double xx = x0 / a2 * (1.0 - y0 / r0), yy = y0 / b2 * (1.0 - x0 / r0);
+	v[sym_idx(A, A)] += f * xx;
+	v[sym_idx(B, B)] += f * yy;
+	v[sym_idx(C, C)] -= f * (xx + yy);
+	v[sym_idx(A, B)] += f / r0;
+	v[sym_idx(A, C)] += f * z / a2 * (1.0 - y0 / r0);
+	v[sym_idx(B, C)] += f * z / b2 * (1.0 - x0 / r0);
+}
+
+// f d_A d_a d_b (1 / r) at r = P, added (the derivative along A of d_a d_b (1 / r)).
+__device__ void line_derivative(const double P[3], int A, double f, double *v)
+{
+	const double r2 = P[0] * P[0] + P[1] * P[1] + P[2] * P[2];
+	const double ir = rsqrt(r2), ir5 = ir * ir * ir * ir * ir, ir7 = ir5 * ir * ir;
+	const int ab[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+	for (int c = 0; c < 6; ++c) {
+		const int a = ab[c][0], b = ab[c][1];
+		double t = -15.0 * P[a] * P[b] * P[A] * ir7;
+		if (a == b) t += 3.0 * P[A] * ir5;
+		if (a == A) t += 3.0 * P[b] * ir5;
+		if (b == A) t += 3.0 * P[a] * ir5;
+		v[c] += f * t;
+	}
+}
+
+// The images P + r L e_A for r >= TAIL_M, in place of their sum: the midpoint rule with its first
+// Euler-Maclaurin correction, L^-1 int_{s_M}^inf f + (L / 24) d_A f(s_M), s_M = P + (TAIL_M - 1/2) L e_A
+// (the next term is below 1e-9 of the sum).
+__device__ void line_continuum(double P[3], int A, double L, double V4, double *v)
+{
+	const double p0 = P[A];
+	P[A] = p0 + (TAIL_M - 0.5) * L;
+	line_integral(P, A, V4 / L, v);
+	line_derivative(P, A, V4 * L / 24.0, v);
+	P[A] = p0;
+}
+
+// Images P + r L e_A, r >= 0 (point dipoles of one cell).
+__device__ void line_tail(double P[3], int A, double L, double V4, double *v)
+{
+	const double p0 = P[A];
+	for (int r = 0; r < TAIL_M; ++r) {
+		P[A] = p0 + r * L;
+		point_dipole(P, V4, v);
+	}
+	P[A] = p0;
+	line_continuum(P, A, L, V4, v);
+}
+
+// Images P + r L_A e_A + s L_B e_B, r, s >= 0.
+__device__ void corner_tail(double P[3], int A, int B, double LA, double LB, double V4, double *v)
+{
+	const double pa = P[A], pb = P[B];
+	for (int s = 0; s < TAIL_M; ++s) {
+		P[B] = pb + s * LB;
+		for (int r = 0; r < TAIL_M; ++r) {
+			P[A] = pa + r * LA;
+			point_dipole(P, V4, v);
+		}
+		P[A] = pa;
+		line_continuum(P, A, LA, V4, v);
+	}
+	P[B] = pb;
+	for (int r = 0; r < TAIL_M; ++r) {
+		P[A] = pa + r * LA;
+		line_continuum(P, B, LB, V4, v);
+	}
+	P[B] = pb + (TAIL_M - 0.5) * LB;
+	P[A] = pa + (TAIL_M - 0.5) * LA;
+	quadrant_integral(P, A, B, V4 / (LA * LB), v);
+	P[A] = pa;
+	P[B] = pb;
+}
+
+// Sum over images of the negated tensor of source offset (i, j, k), halved for each coordinate
+// at zero displacement, plus the far images (tails); out[6] per source offset.
+__global__ void __launch_bounds__(128) k_tensor_images(int nx, int ny, int nz, double dx, double dy, double dz,
+                                                       int Rx, int Ry, int Rz, int tails,
+                                                       const double *__restrict__ glx,
+                                                       const double *__restrict__ glw, double *__restrict__ out)
+{
+	const size_t cnt = (size_t)nx * ny * nz;
+	const int n3[3] = {nx, ny, nz}, R3[3] = {Rx, Ry, Rz};
+	const double d3[3] = {dx, dy, dz};
+	const double V4 = dx * dy * dz / (4.0 * PI);
+	for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
+		const int ijk[3] = {(int)(q % nx), (int)((q / nx) % ny), (int)(q / ((size_t)nx * ny))};
+		double S[6] = {0, 0, 0, 0, 0, 0};
+		for (int rz = 0; rz < Rz; ++rz)
+			for (int ry = 0; ry < Ry; ++ry)
+				for (int rx = 0; rx < Rx; ++rx) {
+					const int I = ijk[0] + rx * nx, J = ijk[1] + ry * ny, K = ijk[2] + rz * nz;
+					const double w = (I == 0 ? 0.5 : 1.0) * (J == 0 ? 0.5 : 1.0) * (K == 0 ? 0.5 : 1.0);
+					double v[6];
+					const bool touching = I <= 1 && J <= 1 && K <= 1;
+					if (touching || !tensor_quad(I, J, K, dx, dy, dz, glx, glw, v)) tensor_newell(I, J, K, dx, dy, dz, v);
+					for (int c = 0; c < 6; ++c) S[c] += w * v[c];
+				}
+		if (tails) {
+			// one periodic axis beyond its repetitions, the others within theirs (tensor.cpp:60-104)
+			for (int A = 0; A < 3; ++A) {
+				if (R3[A] <= 1) continue;
+				const int B = (A + 1) % 3, C = (A + 2) % 3;
+				for (int rc = 0; rc < R3[C]; ++rc)
+					for (int rb = 0; rb < R3[B]; ++rb) {
+						const int IB = ijk[B] + rb * n3[B], IC = ijk[C] + rc * n3[C];
+						const double w = (IB == 0 ? 0.5 : 1.0) * (IC == 0 ? 0.5 : 1.0);
+						double P[3];
+						P[A] = (ijk[A] + R3[A] * n3[A]) * d3[A];
+						P[B] = IB * d3[B];
+						P[C] = IC * d3[C];
+						double v[6] = {0, 0, 0, 0, 0, 0};
+						line_tail(P, A, n3[A] * d3[A], V4, v);
+						for (int c = 0; c < 6; ++c) S[c] += w * v[c];
+					}
+			}
+			// two periodic axes beyond their repetitions (tensor.cpp:105-161)
+			for (int A = 0; A < 3; ++A)
+				for (int B = A + 1; B < 3; ++B) {
+					if (R3[A] <= 1 || R3[B] <= 1) continue;
+					const int C = 3 - A - B;
+					for (int rc = 0; rc < R3[C]; ++rc) {
+						const int IC = ijk[C] + rc * n3[C];
+						const double w = IC == 0 ? 0.5 : 1.0;
+						double P[3];
+						P[A] = (ijk[A] + R3[A] * n3[A]) * d3[A];
+						P[B] = (ijk[B] + R3[B] * n3[B]) * d3[B];
+						P[C] = IC * d3[C];
+						double v[6] = {0, 0, 0, 0, 0, 0};
+						corner_tail(P, A, B, n3[A] * d3[A], n3[B] * d3[B], V4, v);
+						for (int c = 0; c < 6; ++c) S[c] += w * v[c];
+					}
+				}
+		}
+		for (int c = 0; c < 6; ++c) out[6 * q + c] = S[c];
+	}
+}
+
+// Every entry (I, J, K) of the padded tensor gathers its sources of the eight octants: along an
+// axis, octant o = +-1 reads source offset (o I + e) mod e when that is below n (tensor.cpp:166-180
+// scatters the same sums), with the parity signs of the off-diagonal components.
+__global__ void __launch_bounds__(128) k_tensor_gather(int nx, int ny, int nz, int ex, int ey, int ez,
+                                                       const double *__restrict__ S, double *__restrict__ out)
+{
+	const size_t cnt = (size_t)ex * ey * ez;
+	for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cnt; q += (size_t)gridDim.x * blockDim.x) {
+		const int I = (int)(q % ex), J = (int)((q / ex) % ey), K = (int)(q / ((size_t)ex * ey));
+		double acc[6] = {0, 0, 0, 0, 0, 0};
+		for (int o = -1; o <= 1; o += 2) {
+			const int i = (o * I + ex) % ex;
+			if (i >= nx) continue;
+			for (int p = -1; p <= 1; p += 2) {
+				const int j = (p * J + ey) % ey;
+				if (j >= ny) continue;
+				for (int r = -1; r <= 1; r += 2) {
+					const int k = (r * K + ez) % ez;
+					if (k >= nz) continue;
+					const double *s = S + 6 * (((size_t)k * ny + j) * nx + i);
+					acc[0] += s[0];
+					acc[1] += o * p * s[1];
+					acc[2] += o * r * s[2];
+					acc[3] += s[3];
+					acc[4] += p * r * s[4];
+					acc[5] += s[5];
+				}
+			}
+		}
+		for (int c = 0; c < 6; ++c) out[6 * q + c] = acc[c];
+	}
+}
+
 } // namespace
 } // namespace mm
 
@@ -298,6 +530,39 @@ MM_API mm_status mm_demag_tensor(int nx, int ny, int nz, double dx, double dy, d
 	const int grid = (int)(want < 65535u * 16 ? want : 65535u * 16);
 	k_demag_tensor<<<grid, 128, 0, st>>>(nx, ny, nz, dx, dy, dz, ex, ey, ez, gl->x, gl->w, N_out);
 	return after_launch("k_demag_tensor");
+}
+
+MM_API mm_status mm_demag_tensor_periodic(int nx, int ny, int nz, double dx, double dy, double dz, int pbc_x,
+                                          int pbc_y, int pbc_z, int repeat, int ex, int ey, int ez, double *N_out,
+                                          void *stream)
+{
+	if (nx <= 0 || ny <= 0 || nz <= 0 || !(dx > 0) || !(dy > 0) || !(dz > 0) || !N_out || repeat < 1)
+		return fail(MM_ERR_INVALID_ARGUMENT, "mm_demag_tensor_periodic: invalid argument");
+	const int n3[3] = {nx, ny, nz}, e3[3] = {ex, ey, ez}, pb[3] = {pbc_x, pbc_y, pbc_z};
+	for (int a = 0; a < 3; ++a)
+		if (pb[a] ? e3[a] != n3[a] : e3[a] < 2 * n3[a] - 1)
+			return fail(MM_ERR_INVALID_ARGUMENT, "mm_demag_tensor_periodic: a periodic axis needs e == n, the "
+			                                     "others e >= 2n - 1 (round_tensor_dimension)");
+	if (!pbc_x && !pbc_y && !pbc_z) return mm_demag_tensor(nx, ny, nz, dx, dy, dz, ex, ey, ez, N_out, stream);
+	cudaStream_t st = as_stream(stream);
+	GLTable *gl = nullptr;
+	MM_TRY(gl_table(&gl));
+	const size_t cnt = (size_t)nx * ny * nz;
+	double *S = nullptr;
+	MM_CUDA(cudaMallocAsync(&S, 6 * cnt * sizeof(double), st));
+	const char *off = std::getenv("MAGNUM_DEMAG_NO_INFINITY_CORRECTION");  // tensor.cpp:45
+	const int Rx = pbc_x ? repeat : 1, Ry = pbc_y ? repeat : 1, Rz = pbc_z ? repeat : 1;
+	const size_t want = (cnt + 127) / 128;
+	k_tensor_images<<<(int)(want < 65535u * 16 ? want : 65535u * 16), 128, 0, st>>>(
+	    nx, ny, nz, dx, dy, dz, Rx, Ry, Rz, off ? 0 : 1, gl->x, gl->w, S);
+	mm_status r = after_launch("k_tensor_images");
+	if (r == MM_OK) {
+		const size_t out = (size_t)ex * ey * ez, w2 = (out + 127) / 128;
+		k_tensor_gather<<<(int)(w2 < 65535u * 16 ? w2 : 65535u * 16), 128, 0, st>>>(nx, ny, nz, ex, ey, ez, S, N_out);
+		r = after_launch("k_tensor_gather");
+	}
+	cudaFreeAsync(S, st);
+	return r;
 }
 
 } // extern "C"

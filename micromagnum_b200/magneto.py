@@ -723,25 +723,23 @@ def round_tensor_dimension(dim: int, periodic: bool, padding: int) -> int:
 
 def GenerateDemagTensor(nx, ny, nz, dx, dy, dz, px, py, pz, repeat, padding, cache_dir=None) -> Matrix:
     """bindings/mmm/demag.i:27-42 (mmm/demag/demag_tensor.cpp:116-186), computed on the GPU in FP64.
-    Returns Matrix(Shape(6, ex, ey, ez)) holding the negated tensor (float64 in either mode).
-    Periodic meshes are not supported by the GPU generator (RuntimeError).  With a cache
-    directory, a tensor stored there under the reference's file name (demag_tensor.cpp:52-73) is
-    loaded instead, and a computed one is stored when its generation took longer than 30 s, the
-    reference's rule (demag_tensor.cpp:178-181); the file is the raw float64 array, as the
-    reference writes it."""
+    Returns Matrix(Shape(6, ex, ey, ez)) holding the negated tensor (float64 in either mode); along
+    periodic axes (px, py, pz) no padding and `repeat` periodic images plus the images beyond them
+    (mm_demag_tensor_periodic).  With a cache directory, a tensor stored there under the
+    reference's file name (demag_tensor.cpp:52-73) is loaded instead, and a computed one is stored
+    when its generation took longer than 30 s, the reference's rule (demag_tensor.cpp:178-181); the
+    file is the raw float64 array, as the reference writes it."""
     ex = round_tensor_dimension(nx, px, padding)
     ey = round_tensor_dimension(ny, py, padding)
     ez = round_tensor_dimension(nz, pz, padding)
     N = Matrix(Shape(6, ex, ey, ez), _fixed_dtype=torch.float64)
-    if px or py or pz:
-        raise RuntimeError("GenerateDemagTensor: periodic boundaries are not supported on the GPU; "
-                           "pass a tensor to SymmetricMatrixVectorConvolution_FFT instead")
     path = demag_cache_file(nx, ny, nz, ex, ey, ez, dx, dy, dz, px, py, pz, repeat, cache_dir) if cache_dir else None
     if path and os.path.exists(path) and os.path.getsize(path) == 8 * N.size():
         N.data.copy_(torch.from_numpy(np.fromfile(path, dtype=np.float64)))
         return N
     t0 = time.perf_counter()
-    check(lib().mm_demag_tensor(nx, ny, nz, dx, dy, dz, ex, ey, ez, _ptr(N.data), _stream()))
+    check(lib().mm_demag_tensor_periodic(nx, ny, nz, dx, dy, dz, int(bool(px)), int(bool(py)), int(bool(pz)),
+                                         int(repeat), ex, ey, ez, _ptr(N.data), _stream()))
     torch.cuda.current_stream().synchronize()
     if path and time.perf_counter() - t0 > CACHE_AFTER_S and not os.path.exists(path):
         tmp = f"{path}.{os.getpid()}.tmp"

@@ -32,7 +32,8 @@ TABLEAUS = {"rkf45": _lib.MM_RK_RKF45, "cc45": _lib.MM_RK_CC45, "dp54": _lib.MM_
 
 class RectangularMesh(_magneto.RectangularMesh):
     """magnum.mesh.RectangularMesh (src/magnum/mesh/rectangular_mesh.py:22-35): the mesh from
-    the number of cells and the cell size; the solver itself is non-periodic."""
+    the number of cells and the cell size, with periodic directions ("x", "xy", ...) and their
+    repetitions."""
 
     def __init__(self, num_nodes, cell_size, periodic_bc: str = "", periodic_repeat=None):
         nx, ny, nz = (int(v) for v in num_nodes)
@@ -70,7 +71,8 @@ def _stream_ptr():
 class Solver:
     """Micromagnetic solver on one GPU.
 
-    mesh       : RectangularMesh (non-periodic)
+    mesh       : RectangularMesh; its periodic directions make the exchange stencil wrap around
+                 and the demag tensor periodic (repetitions from the mesh)
     materials  : list of Material (<= 256); regions selects one per cell
     regions    : None (all cells material 0) or uint8 array of nx*ny*nz region indices
     terms      : iterable of "demag", "exchange", "uniaxial", "cubic", "zhangli", "zeeman"
@@ -109,6 +111,10 @@ class Solver:
             cfg.H_ext[q], cfg.H_pulse[q] = H_ext[q], H_pulse[q]
         cfg.pulse_rise = pulse_rise
         cfg.fsal_reuse_after_reject = int(fsal_reuse_after_reject)
+        pbc, reps = mesh.periodic_bc
+        for q, axis in enumerate("xyz"):
+            cfg.pbc[q] = int(axis in pbc)
+        cfg.pbc_repeat = int(reps) if pbc else 0
         self.cfg = cfg
         self.precision = precision
         mats = (_lib.mm_material * len(materials))(*[m.to_c() for m in materials])

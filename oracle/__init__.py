@@ -233,14 +233,14 @@ class Solver:
                     ("eps_abs", _D), ("eps_rel", _D), ("h0", _D),
                     ("H_ext", _D * 3), ("H_pulse", _D * 3), ("pulse_rise", _D),
                     ("fsal_reuse_after_reject", ctypes.c_int), ("float_norm", ctypes.c_int),
-                    ("use_fft", ctypes.c_int)]
+                    ("use_fft", ctypes.c_int), ("pbc", ctypes.c_int * 3)]
 
     def __init__(self, dims, delta, Ms, A=0.0, alpha=0.0, k_uniaxial=0.0, k_cubic=0.0,
                  axis1=(0, 0, 0), axis2=(0, 0, 0), P=0.0, xi=0.0, j=(0, 0, 0),
                  terms=("demag", "exchange"), evolver="dp54", eps_abs=1e-3, eps_rel=1e-4, h0=1e-13,
                  do_precess=True, zl_do_precess=True, H_ext=(0, 0, 0), H_pulse=(0, 0, 0),
                  pulse_rise=0.0, fsal_reuse_after_reject=True, float_norm=True, use_fft=None,
-                 tensor=None, padding=2):
+                 tensor=None, padding=2, pbc=(0, 0, 0)):
         self.L = restated()
         nx, ny, nz = dims
         n = nx * ny * nz
@@ -263,6 +263,8 @@ class Solver:
         c.fsal_reuse_after_reject = int(fsal_reuse_after_reject)
         c.float_norm = int(float_norm)
         c.use_fft = int(use_fft if use_fft is not None else n > 8192)
+        for q in range(3):
+            c.pbc[q] = int(bool(pbc[q]))
         self.cfg = c
 
         def cell(v):

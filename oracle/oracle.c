@@ -737,7 +737,8 @@ static void rhs(or_solver *s, const double *M, double t, double *dMdt, double *H
 		add_to(H, s->Htmp, n3);
 	}
 	if (c->terms & 2) {
-		or_exchange(c->nx, c->ny, c->nz, c->dx, c->dy, c->dz, 0, 0, 0, s->Ms, s->A, M, s->Htmp);
+		or_exchange(c->nx, c->ny, c->nz, c->dx, c->dy, c->dz, c->pbc[0], c->pbc[1], c->pbc[2], s->Ms, s->A, M,
+		            s->Htmp);
 		add_to(H, s->Htmp, n3);
 	}
 	if (c->terms & 4) {

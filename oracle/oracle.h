@@ -63,6 +63,8 @@ typedef struct {
 	int fsal_reuse_after_reject;
 	int float_norm;         /* 1: CPU normalize3 (norm from float-cast components) */
 	int use_fft;            /* 1: FFT convolution, 0: direct summation */
+	int pbc[3];             /* periodic exchange along x, y, z (exchange_cpu.cpp:141-235); the
+	                           tensor passed in carries the periodic demag images */
 } or_solver_config;
 
 /* Per-cell parameters (arrays of N; vectors SoA).  tensor: (6, ex, ey, ez) as above. */

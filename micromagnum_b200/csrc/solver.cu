@@ -179,14 +179,29 @@ __device__ __forceinline__ V3<T> zeeman_field(const CellArgs<T> &a, double t)
 // Field terms and dm/dt of one non-empty cell (material M, unit state m) from its gathered
 // neighbourhood: nb[q] / nms[q] are the unit state and Ms of the neighbours x-1, x+1, y-1, y+1,
 // z-1, z+1 (zero where the neighbour is outside the box).  Hd: demag field, Hz: applied field.
-template <typename T>
+// Whether term t is on: a compile-time answer when the kernel was specialised for the term set TM
+// (TM >= 0), else the run-time bit set.
+template <int TM, typename T>
+__device__ __forceinline__ bool term_on(const CellArgs<T> &a, int t)
+{
+	if constexpr (TM >= 0) return (TM & t) != 0;
+	else return (a.terms & t) != 0;
+}
+
+// Term sets the staged stage kernel is compiled for (besides the run-time one): the granular
+// slab's and the thin film's.
+constexpr int TM_RUNTIME = -1;
+constexpr int TM_SLAB = MM_TERM_DEMAG | MM_TERM_EXCHANGE | MM_TERM_UNIAXIAL | MM_TERM_ZHANGLI;
+constexpr int TM_FILM = MM_TERM_DEMAG | MM_TERM_EXCHANGE;
+
+template <typename T, int TM = TM_RUNTIME>
 __device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> &M, const V3<T> &m,
                                           const V3<T> (&nb)[6], const T (&nms)[6], int x, int yy, int z,
                                           V3<T> Hd, V3<T> Hz, V3<T> &Heff, V3<T> &dm)
 {
 	const T ms = M.Ms;
-	V3<T> H = (a.terms & MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0);
-	if (a.terms & MM_TERM_EXCHANGE) {
+	V3<T> H = term_on<TM>(a, MM_TERM_DEMAG) ? Hd : v3<T>(0, 0, 0);
+	if (term_on<TM>(a, MM_TERM_EXCHANGE)) {
 		// exchange_cpu.cpp:60-139: H = 2A/(mu0 Ms) sum_nb w (m_nb - m), empty neighbours skipped
 		const T w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
 		V3<T> sum = v3<T>(0, 0, 0);
@@ -195,12 +210,12 @@ __device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> 
 			if (nms[q] != T(0)) sum = sum + w[q] * (nb[q] - m);
 		H = H + M.cex * sum;
 	}
-	if (a.terms & MM_TERM_UNIAXIAL) {
+	if (term_on<TM>(a, MM_TERM_UNIAXIAL)) {
 		// anisotropy_cpu.cpp:29-73 (k == 0 gives ku == 0)
 		const V3<T> ax = v3<T>(M.a1[0], M.a1[1], M.a1[2]);
 		H = H + (M.ku * dot(m, ax)) * ax;
 	}
-	if (a.terms & MM_TERM_CUBIC) {
+	if (term_on<TM>(a, MM_TERM_CUBIC)) {
 		// anisotropy_cpu.cpp:75-119 on m/|m|
 		const T len = sqrt(dot(m, m));
 		const V3<T> u = len > T(0) ? (T(1) / len) * m : v3<T>(0, 0, 0);
@@ -215,7 +230,7 @@ __device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> 
 	// llge_cpu.cpp:25-45 on unit m
 	const V3<T> mxh = cross(m, H);
 	dm = M.l1 * mxh + M.l2 * cross(m, mxh);
-	if (a.terms & MM_TERM_ZHANGLI) {
+	if (term_on<TM>(a, MM_TERM_ZHANGLI)) {
 		// fdm_zhangli_cpu.cpp:100-200: u = (j.grad)M from raw M = Ms m (no Ms masking),
 		// one-sided at the borders, zero along a dimension of size 1
 		const V3<T> Mc = scale_rn(ms, m);
@@ -557,7 +572,7 @@ inline bool stage_tma_fits(int nx, size_t esize, bool regions)
 	return (nx * esize) % 16 == 0 && (!regions || nx % 16 == 0);
 }
 
-template <typename T, bool COMP, int S>
+template <typename T, bool COMP, int S, int TM>
 __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
     k_stage_tma(const __grid_constant__ StageMaps maps, CellArgs<T> a, StageCoef sc, const KTab<T> *__restrict__ ktab,
                 T *__restrict__ y_out, T *__restrict__ y_out_lo, DevState *__restrict__ st, int tiles_x,
@@ -572,7 +587,7 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 	unsigned char *ys = smem_st;
 	uint8_t *rs = smem_st + G::YB;
 	T *os = reinterpret_cast<T *>(smem_st + G::YB + G::RB);
-	const bool demag = a.terms & MM_TERM_DEMAG;
+	const bool demag = term_on<TM>(a, MM_TERM_DEMAG);
 	int kop[MAXS], op_hd, op_hi, op_lo;
 	const int nops = stage_ops(sc, S, COMP, demag, kop, op_hd, op_hi, op_lo);
 	// barriers: halo planes arrived [ST_RING], operands arrived [ST_NOB], step done [ST_NOB]
@@ -738,17 +753,17 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 						const int drq[6] = {-1, 1, -ST_XR, ST_XR, 0, 0};
 						V3<T> nb[6];
 						T nms[6];
+						// every neighbour read stays inside the staged planes (the halo past the grid
+						// reads as zero, a missing plane z -+ 1 is a stale ring slot), so the reads
+						// are unconditional and the neighbours outside the box are masked afterwards
 #pragma unroll
 						for (int q = 0; q < 6; ++q) {
-							if (has[q]) {
-								nb[q] = Y3(yq[q], dq[q]);
-								nms[q] = a.reg ? msr[rq[q][drq[q]]] : M.Ms;
-							} else {
-								nb[q] = v3<T>(0, 0, 0);
-								nms[q] = T(0);
-							}
+							const V3<T> v = Y3(yq[q], dq[q]);
+							const T ms_q = a.reg ? msr[rq[q][drq[q]]] : M.Ms;
+							nb[q] = has[q] ? v : v3<T>(0, 0, 0);
+							nms[q] = has[q] ? ms_q : T(0);
 						}
-						cell_core<T>(a, M, m, nb, nms, x, yy, z, hd, Hz, Heff, ki);
+						cell_core<T, TM>(a, M, m, nb, nms, x, yy, z, hd, Hz, Heff, ki);
 					}
 					T *const pk = kS + i, *const py = y_out + i;
 					auto put3 = [&](T *p, V3<T> v) {
@@ -1138,6 +1153,7 @@ struct mm_solver {
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
 	// staged stage kernel: used when the rows are 16-byte aligned; grid and shared memory per stage
 	bool st_tma = false;
+	int st_tm = -1;                  // term set the staged kernel is specialised for (-1: run time)
 	int st_resident = 0;             // resident blocks of k_stage on this solver's device
 	int st_grid[MAXS] = {};
 	size_t st_smem[MAXS] = {};
@@ -1383,10 +1399,12 @@ mm_status stage_tma_prepare(mm_solver *s)
 	MM_CUDA(cudaGetDevice(&dev));
 	MM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
 	if (smem + 2 * 256 * sizeof(T) > (size_t)optin) return fail(MM_ERR_UNSUPPORTED, "staged stage: shared memory");
-	MM_CUDA(cudaFuncSetAttribute(k_stage_tma<T, COMP, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-	                             optin - 2 * 256 * (int)sizeof(T)));
+	const void *fn = s->st_tm == TM_SLAB   ? (const void *)k_stage_tma<T, COMP, S, TM_SLAB>
+	                 : s->st_tm == TM_FILM ? (const void *)k_stage_tma<T, COMP, S, TM_FILM>
+	                                       : (const void *)k_stage_tma<T, COMP, S, TM_RUNTIME>;
+	MM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 2 * 256 * (int)sizeof(T)));
 	int per_sm = 0;
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tma<T, COMP, S>, ST_CONS + 32, smem));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, ST_CONS + 32, smem));
 	if (per_sm < 1) return fail(MM_ERR_UNSUPPORTED, "staged stage kernel does not fit on an SM");
 	const mm_solver_config &c = s->cfg;
 	const long long nsteps = (long long)((c.nx + ST_X - 1) / ST_X) * ((c.ny + ST_Y - 1) / ST_Y) * c.nz;
@@ -1438,6 +1456,9 @@ mm_status stage_tma_setup(mm_solver *s, std::integer_sequence<int, S...>)
 	const bool periodic = s->cfg.pbc[0] || s->cfg.pbc[1] || s->cfg.pbc[2];
 	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr) && !(env && env[0] == '0') && !periodic;
 	if (!s->st_tma) return MM_OK;
+	s->st_tm = s->cfg.terms == TM_SLAB ? TM_SLAB : s->cfg.terms == TM_FILM ? TM_FILM : TM_RUNTIME;
+	if (const char *gen = std::getenv("MMB200_STAGE_GENERIC"))  // the run-time term set (comparison tests)
+		if (gen[0] == '1') s->st_tm = TM_RUNTIME;
 	mm_status r = stage_tma_maps<T>(s);
 	((r = (r == MM_OK && S < s->tab.s) ? stage_tma_prepare<T, COMP, S>(s) : r), ...);
 	if (r != MM_OK) {
@@ -1457,8 +1478,16 @@ void stage_tma_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef 
 	maps.yin = s->st_yin[yin == (const T *)s->ys[0] ? 1 : (yin == (const T *)s->ys[1] ? 2 : 0)];
 	(void)yhi;
 	(void)ylo;
-	k_stage_tma<T, COMP, S><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
-	    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, (c.nx + ST_X - 1) / ST_X, (c.ny + ST_Y - 1) / ST_Y);
+	const int tx = (c.nx + ST_X - 1) / ST_X, ty = (c.ny + ST_Y - 1) / ST_Y;
+	if (s->st_tm == TM_SLAB)
+		k_stage_tma<T, COMP, S, TM_SLAB><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+		    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
+	else if (s->st_tm == TM_FILM)
+		k_stage_tma<T, COMP, S, TM_FILM><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+		    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
+	else
+		k_stage_tma<T, COMP, S, TM_RUNTIME><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+		    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
 }
 
 template <typename T, bool COMP>

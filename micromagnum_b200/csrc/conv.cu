@@ -691,7 +691,7 @@ __device__ __forceinline__ void z_reg_body(cplx<T> *__restrict__ S, const T *__r
 }
 
 template <typename T, int PZ>
-__global__ void __launch_bounds__(ZR_THREADS, 3) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
+__global__ void __launch_bounds__(ZR_THREADS, 2) k_z_reg(cplx<T> *__restrict__ S, const T *__restrict__ Nt, int nz,
                                                         int py, int hx, int lx, int qy, int qz)
 {
 	z_reg_body<T, PZ>(S, Nt, nz, py, hx, lx, qy, qz, blockIdx.x, blockIdx.y);
@@ -721,6 +721,9 @@ struct YTmaGeom {
 	static constexpr uint32_t TILE_BYTES = (uint32_t)(TB * ROWS * sizeof(C));
 	static constexpr size_t WORK = ((size_t)SmCols<N, TB, 4>::SIZE * sizeof(C) + 15) / 16 * 16;
 	static constexpr size_t SMEM = 2 * (size_t)TILE_BYTES + WORK + 16;
+	// the single-instance pass keeps the twiddle table W_N^k in shared memory behind the barriers
+	static constexpr size_t TW = SMEM;
+	static constexpr size_t SMEM_TW = SMEM + (size_t)N * sizeof(C);
 };
 
 // Columns per CTA of the single-instance TMA y pass: 32-byte rows, at most 256 threads, so that
@@ -748,6 +751,8 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * (size_t)G::TILE_BYTES + G::WORK);
 	const int tid = threadIdx.x;
 	const int line = tid & (TB - 1), j0 = tid / TB;
+	C *tws = reinterpret_cast<C *>(smem_tma + G::TW);
+	for (int q = tid; q < N; q += blockDim.x) tws[q] = twN[q];
 	auto issue = [&](int t, int b) {
 		const int tx = t % tiles_x, plane = t / tiles_x;
 		C *dst = b ? stage1 : stage0;
@@ -796,8 +801,8 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 				issue(next, b);
 			}
 		};
-		if constexpr (INV) cta_fft<T, N, R, TB, INV, SI>(work, twN, line, j0, ld, st, release);
-		else cta_fft_h0<T, N, R, TB, SI>(work, twN, line, j0, ld, st, release);  // rows >= N/2 are zero
+		if constexpr (INV) cta_fft<T, N, R, TB, INV, SI>(work, tws, line, j0, ld, st, release);
+		else cta_fft_h0<T, N, R, TB, SI>(work, tws, line, j0, ld, st, release);  // rows >= N/2 are zero
 	}
 }
 
@@ -815,8 +820,12 @@ struct XTmaGeom {
 	// staged rows (at most 2 LPB spectrum rows of N/2 + 1 + padding complex values) fit in WORK
 	// with room to spare for N >= 64; shorter rows use the non-staged kernels
 	static constexpr size_t BUF = (WORK + 127) / 128 * 128;
-	static constexpr size_t SMEM = 2 * BUF + 16 + 256 * (sizeof(C) / 2);  // + the forward pass's Ms table
-	static constexpr int MINB = (3 * SMEM <= 227 * 1024 && THREADS <= 256) ? 3 : (2 * SMEM <= 227 * 1024 ? 2 : 1);
+	// + the forward pass's Ms table and its twiddle table W_N^k (read once per persistent CTA, so
+	// that its butterflies' twiddles come from shared memory; the inverse pass reads them from
+	// global memory, which measured slightly faster there)
+	static constexpr size_t TW = 2 * BUF + 16 + 256 * (sizeof(C) / 2);
+	static constexpr size_t SMEM = TW + (size_t)N * sizeof(C);
+	static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;
 };
 
 // Forward: with SCALE the tile's region bytes (rows r % (ny nz), contiguous within a tile) ride
@@ -847,6 +856,8 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 	};
 	if (SCALE)
 		for (int r = tid; r < 256; r += blockDim.x) msr[r] = ms_tab[r];
+	C *tws = reinterpret_cast<C *>(smem_tma + G::TW);
+	for (int q = tid; q < N; q += blockDim.x) tws[q] = twN[q];
 	if (tid == 0) {
 		mbar_init(&bar[0], 1);
 		mbar_init(&bar[1], 1);
@@ -887,7 +898,7 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 			return C{a, bb};
 		};
 		auto st = [&](int l, int kk, C v) { sm[SI::at(l, kk)] = v; };
-		cta_fft_h0<T, N, G::R, LPB, SI, true>(sm, twN, line, j0, ld, st);  // x >= nx, N/2 <= x: zero
+		cta_fft_h0<T, N, G::R, LPB, SI, true>(sm, tws, line, j0, ld, st);  // x >= nx, N/2 <= x: zero
 		__syncthreads();
 		C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
 		C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
@@ -1010,16 +1021,16 @@ mm_status fs_setup_y_tma(ConvPlan *p)
 	using GF = YTmaGeom<N, TB, false, C>;
 	using GI = YTmaGeom<N, TB, true, C>;
 	p->tma_y = false;
-	if (GI::SMEM > 227 * 1024 || 2 * p->ny > p->py || TB * sizeof(C) < 16) return MM_OK;
+	if (GI::SMEM_TW > 227 * 1024 || 2 * p->ny > p->py || TB * sizeof(C) < 16) return MM_OK;
 	constexpr int E = GF::E;
 	const uint64_t d0 = (uint64_t)p->lx * E, rowb = (uint64_t)p->lx * sizeof(C), planeb = rowb * p->py;
 	MM_TRY(tma_encode_3d(&p->tm_yf, p->spec, d0, (uint64_t)p->ny, 3ull * p->nz, rowb, planeb, TB * E, GF::BR, 1));
 	MM_TRY(tma_encode_3d(&p->tm_yi, p->spec, d0, (uint64_t)p->py, 3ull * p->nz, rowb, planeb, TB * E, GI::BR, 1));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, false>, GF::SMEM));
-	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, true>, GI::SMEM));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, false>, GF::SMEM_TW));
+	MM_TRY(set_smem<T>((const void *)k_y_tma<T, N, TB, true>, GI::SMEM_TW));
 	int bf = 0, bi = 0;
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, TB, false>, THREADS, GF::SMEM));
-	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, TB, true>, THREADS, GI::SMEM));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bf, k_y_tma<T, N, TB, false>, THREADS, GF::SMEM_TW));
+	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bi, k_y_tma<T, N, TB, true>, THREADS, GI::SMEM_TW));
 	if (bf < 1 || bi < 1) return MM_OK;
 	p->grid_yf = bf * num_sms();
 	p->grid_yi = bi * num_sms();
@@ -1039,7 +1050,7 @@ void fs_y_tma(ConvPlan *p, cudaStream_t st)
 	using G = YTmaGeom<N, TB, INV, C>;
 	const int tiles_x = (p->hx + TB - 1) / TB, ntiles = tiles_x * 3 * p->nz;
 	const int grid = std::min(ntiles, INV ? p->grid_yi : p->grid_yf);
-	k_y_tma<T, N, TB, INV><<<grid, THREADS, G::SMEM, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
+	k_y_tma<T, N, TB, INV><<<grid, THREADS, G::SMEM_TW, st>>>(INV ? p->tm_yi : p->tm_yf, (C *)p->spec,
 	                                                       INV ? p->ny : N, p->hx, p->lx, tiles_x, ntiles,
 	                                                       (const C *)p->tw_y, p->err);
 }

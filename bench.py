@@ -419,15 +419,47 @@ def batch_instances(count, seed):
     return out, M0
 
 
+def fp64_solve(q, M0, max_torque=1e-4, cap_s=None, chunk=256):
+    """One instance solved alone by the plain FP64 solver (the same geometry, mask, materials,
+    controller and stop rule as in the batch), from its initial state to the end: integrated to
+    q.t_end when it has one, else relaxed to max |m x H| / Ms < max_torque checked after every
+    step.  Runs in chunks (256 steps, or a tenth of t_end) and gives up once cap_s device seconds
+    are spent.  Returns (device seconds, accepted steps, finished); solver creation (tensor, plan)
+    is not timed, as the batch's is not."""
+    import torch
+    from micromagnum_b200.solver import Material, RectangularMesh, Solver
+    mats = [Material(Ms=0.0, A=0.0, alpha=q.alpha), Material(Ms=q.Ms, A=q.A, alpha=q.alpha)]
+    s = Solver(RectangularMesh(q.dims, q.delta), mats, regions=q.mask, terms=("demag", "exchange", "zeeman"),
+               precision="f64", evolver="dp54", eps_abs=1e-3, eps_rel=1e-4, padding=4, H_ext=q.H_ext,
+               H_pulse=q.H_pulse, pulse_rise=q.pulse_rise)
+    s.M = M0
+    torch.cuda.synchronize()
+    sec, done, part = 0.0, False, 0
+    while not done and (cap_s is None or sec < cap_s):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        if q.t_end > 0:
+            part += 1
+            s.solve(q.t_end * min(part, 10) / 10)
+            done = part >= 10
+        else:
+            done = s.relax_torque(max_torque=max_torque, check_every_nth_step=1, max_steps=chunk)
+        e1.record()
+        torch.cuda.synchronize()
+        sec += e0.elapsed_time(e1) * 1e-3
+    steps = s.stats["steps"]
+    s.close()
+    return sec, steps, done
+
+
 def run_batch(args):
-    """Relaxes the 256 instances in lock-step rounds until all finish or the device-time budget
-    runs out.  The FP64 baseline is the plain FP64 single-instance solver, one instance at a time:
-    for every instance the batch finished, its FP64 time per accepted step is measured over a few
-    steps from the same initial state and multiplied by the step count the solve needed."""
+    """Relaxes the instances in lock-step rounds until all finish (or the device-time budget runs
+    out, which the line states).  The FP64 baseline is measured, not extrapolated: a seeded sample
+    of the same instances is solved one at a time, each from its initial state to the end, by the
+    plain FP64 solver; FP64 solves/s = finished sample solves / their device time."""
     import torch
     from micromagnum_b200 import _lib
     from micromagnum_b200.batch import Batch
-    from micromagnum_b200.solver import Material, RectangularMesh, Solver
 
     insts, M0 = batch_instances(args.batch_count, BATCH_SEED)
     cells = sum(q.n for q in insts)
@@ -436,7 +468,7 @@ def run_batch(args):
     for i, M in enumerate(M0):
         b.set_M(i, M)
     torch.cuda.synchronize()
-    ms, rounds, done = 0.0, 0, 0
+    ms, rounds, done, progress = 0.0, 0, 0, []
     l0 = _lib.launches()
     while rounds < args.batch_rounds and ms * 1e-3 < args.batch_budget:
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -447,7 +479,10 @@ def run_batch(args):
         ms += e0.elapsed_time(e1)
         rounds += r
         res = b.results()
-        done = sum(1 for x in res if x["status"] == 1)
+        d = sum(1 for x in res if x["status"] == 1)
+        if d // 16 != done // 16:
+            progress.append([round(ms * 1e-3, 2), d])
+        done = d
         if done + sum(1 for x in res if x["status"] == 2) == len(insts):
             break
     launches = _lib.launches() - l0
@@ -456,30 +491,16 @@ def run_batch(args):
     finished = [i for i, x in enumerate(res) if x["status"] == 1]
     b.close()
 
-    # plain FP64, one instance at a time: each instance's FP64 time per accepted step (measured over
-    # a few steps from its initial state) x the accepted steps the batch made for it, finished or not
-    idx = list(range(len(insts)))
-    if args.batch_sample < len(idx):
-        idx = sorted(np.random.default_rng(BATCH_SEED + 2).choice(len(idx), size=args.batch_sample,
-                                                                  replace=False).tolist())
-    t64, steps_b = [], []
+    # plain FP64, one at a time, each to completion
+    idx = sorted(np.random.default_rng(BATCH_SEED + 2).choice(len(insts), size=min(args.batch_sample, len(insts)),
+                                                              replace=False).tolist())
+    t64, steps64, done64 = [], [], 0
     for i in idx:
-        q = insts[i]
-        mats = [Material(Ms=0.0, A=0.0, alpha=q.alpha), Material(Ms=q.Ms, A=q.A, alpha=q.alpha)]
-        s = Solver(RectangularMesh(q.dims, q.delta), mats, regions=q.mask, terms=("demag", "exchange"),
-                   precision="f64", evolver="dp54", eps_abs=1e-3, eps_rel=1e-4, padding=4)
-        s.M = M0[i]
-        s.step()
-        torch.cuda.synchronize()
-        c0 = time.perf_counter()
-        for _ in range(20):
-            s.step()
-        torch.cuda.synchronize()
-        t64.append((time.perf_counter() - c0) / 20)
-        steps_b.append(res[i]["steps"])
-        s.close()
-    scale = sum(x["steps"] for x in res) / max(sum(steps_b), 1)   # sample -> all instances
-    fp64_s = scale * sum(t * k for t, k in zip(t64, steps_b))
+        sec, st, ok = fp64_solve(insts[i], M0[i], max_torque=thr, cap_s=args.batch_budget)
+        t64.append(sec)
+        steps64.append(st)
+        done64 += int(ok)
+    fp64_rate = done64 / sum(t64) if sum(t64) > 0 else None
     value = len(finished) / (ms * 1e-3) if ms > 0 else 0.0
     line = {
         "metric": "batched relax solves/s", "value": value, "unit": "solves/s",
@@ -487,16 +508,24 @@ def run_batch(args):
         "data": "synthetic (seeded sizes, masks, materials, initial m)",
         "config": {"workload": f"{len(insts)} uneven instances, nx,ny in [16,256], nz in {{1,2,4}}, 4 nm cells, "
                                "elliptical masks, relaxed to max |m x H|/Ms < 1e-4, dp54",
-                   "cells_total": cells, "rounds": rounds, "relaxed": len(finished),
-                   "device_time_budget_s": args.batch_budget, "launches_per_round": [first, later]},
+                   "cells_total": cells, "rounds": rounds, "relaxed": len(finished), "instances": len(insts),
+                   "device_time_budget_s": args.batch_budget,
+                   "all_finished": len(finished) == len(insts), "launches_per_round": [first, later]},
         "device_ms": ms, "ms_per_round": ms / max(rounds, 1), "gpu_launches": launches,
+        "relaxed_vs_device_s": progress,
         "accepted_steps": sum(x["steps"] for x in res),
         "cell_rhs_evals_per_s": evals / (ms * 1e-3) if ms > 0 else 0.0,
-        "fp64_one_at_a_time": {"seconds_for_the_same_steps": fp64_s, "instances_timed": len(idx),
-                               "ms_per_step_median": 1e3 * float(np.median(t64)),
-                               "method": "per-instance FP64 time per accepted step (20 steps from the same "
-                                         "initial state) x the accepted steps the batch made for it"},
-        "speedup_vs_fp64_one_at_a_time": fp64_s / (ms * 1e-3) if ms > 0 else None,
+        "fp64_one_at_a_time": {"solves_per_s": fp64_rate, "instances_solved": done64, "instances_timed": len(idx),
+                               "device_s": sum(t64), "accepted_steps": int(sum(steps64)),
+                               "per_instance": [[int(i), list(insts[i].dims), round(t, 3), int(k),
+                                                 int(res[i]["steps"]), int(res[i]["status"])]
+                                                for i, t, k in zip(idx, t64, steps64)],
+                               "per_instance_fields": "index, dims, FP64 device s, FP64 steps, batch steps, "
+                                                      "batch status",
+                               "method": "a seeded sample of the same instances, each solved alone by the plain "
+                                         "FP64 solver from its initial state to the stop rule (device time; solver "
+                                         "creation excluded on both sides)"},
+        "speedup_vs_fp64_one_at_a_time": value / fp64_rate if fp64_rate else None,
     }
     print(json.dumps(line), flush=True)
 
@@ -541,29 +570,6 @@ def serve_requests(count, rate, seed):
     return out
 
 
-def fp64_solve_seconds(req, steps):
-    """Plain FP64 single-instance solver: time per accepted step over a few steps from the
-    request's initial state, times the steps its solve needed."""
-    import torch
-    from micromagnum_b200.solver import Material, RectangularMesh, Solver
-    q = req.instance
-    mats = [Material(Ms=0.0, A=0.0, alpha=q.alpha), Material(Ms=q.Ms, A=q.A, alpha=q.alpha)]
-    s = Solver(RectangularMesh(q.dims, q.delta), mats, regions=q.mask, terms=("demag", "exchange", "zeeman"),
-               precision="f64", evolver="dp54", eps_abs=1e-3, eps_rel=1e-4, padding=4, H_pulse=q.H_pulse,
-               pulse_rise=q.pulse_rise)
-    s.M = req.M0
-    s.step()
-    torch.cuda.synchronize()
-    c0 = time.perf_counter()
-    k = 10
-    for _ in range(k):
-        s.step()
-    torch.cuda.synchronize()
-    dt = (time.perf_counter() - c0) / k
-    s.close()
-    return dt * steps
-
-
 def run_serve(args):
     from micromagnum_b200.serve import Server
     rates = [float(v) for v in args.serve_rates.split(",")]
@@ -576,20 +582,23 @@ def run_serve(args):
         srv.close()
         lat = [c.latency for c in st.completed] or [float("nan")]
         # the same stream served one at a time by the plain FP64 path: a FIFO queue in arrival order
-        # whose solve times are the FP64 time per accepted step x the steps each request needed (the
-        # requests still running at the deadline occupy it for the steps the server made on them, a
-        # lower bound); a request counts as solved when the queue finishes it within the same makespan
+        # whose solve times are measured full FP64 solves (device time, from the request's initial
+        # state to its stop rule); a request counts as solved when the queue finishes it within the
+        # server's makespan, and the queue stops where it passes the makespan (the solve in progress
+        # there is cut at that point, so nothing after it is measured)
         done_ids = {c.id for c in st.completed}
-        t_free, lat64, done64 = 0.0, [], 0
+        t_free, lat64, done64, measured64 = 0.0, [], 0, 0.0
         for r in sorted(reqs, key=lambda r: r.arrival):
-            k = st.progress.get(r.id, 0)
-            if k <= 0:
-                continue
-            if (r.id, k) not in fp64_cache:
-                fp64_cache[(r.id, k)] = fp64_solve_seconds(r, k)
             start = max(t_free, r.arrival)
-            t_free = start + fp64_cache[(r.id, k)]
-            if r.id in done_ids and t_free <= st.makespan:
+            if start >= st.makespan:
+                break
+            cap = st.makespan - start
+            c = fp64_cache.get(r.id)
+            if c is None or (not c[2] and c[0] < cap):
+                c = fp64_cache[r.id] = fp64_solve(r.instance, r.M0, max_torque=SERVE_RELAX_TORQUE, cap_s=cap)
+            measured64 += min(c[0], cap)
+            t_free = start + c[0]
+            if c[2] and t_free <= st.makespan:
                 lat64.append(t_free - r.arrival)
                 done64 += 1
         pt = {
@@ -598,12 +607,11 @@ def run_serve(args):
             "p99_s": float(np.percentile(lat, 99)), "makespan_s": st.makespan, "rounds": st.rounds,
             "peak_resident_gb": st.peak_resident / (1 << 30),
             "fp64_one_at_a_time": {"solves_per_s": done64 / st.makespan if st.makespan > 0 else None,
-                                   "solved": done64, "queue_busy_s": t_free,
+                                   "solved": done64, "measured_device_s": measured64,
                                    "p50_s": float(np.percentile(lat64, 50)) if lat64 else None,
                                    "p99_s": float(np.percentile(lat64, 99)) if lat64 else None,
-                                   "method": "FIFO in arrival order, FP64 time per step x the steps each "
-                                             "request needed (running requests: the steps made by the "
-                                             "deadline), solved = finished within the same makespan"},
+                                   "method": "FIFO in arrival order over measured full FP64 solves (device "
+                                             "time), solved = finished within the server's makespan"},
             "sizes_unfinished": sorted({str(r.instance.dims) for r in reqs if r.id not in done_ids}),
         }
         points.append(pt)
@@ -679,8 +687,9 @@ def main():
     ap.add_argument("--serve-budget", type=float, default=90.0, help="seconds per arrival rate")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--batch-rounds", type=int, default=100000)
-    ap.add_argument("--batch-budget", type=float, default=120.0, help="device seconds for the batched rounds")
-    ap.add_argument("--batch-sample", type=int, default=256, help="instances timed in FP64 for the ratio")
+    ap.add_argument("--batch-budget", type=float, default=900.0, help="device seconds for the batched rounds")
+    ap.add_argument("--batch-sample", type=int, default=16,
+                    help="instances (a seeded sample) solved one at a time in FP64 for the ratio")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32",
                     help="f32: the compensated single-precision form (default); f64: the plain mode")
     ap.add_argument("--dims", default=None, help="override the grid, e.g. 512,512,8 (profiling captures)")

@@ -807,84 +807,106 @@ __global__ void __launch_bounds__(TB * (N / ct_radix(N)), 2)
 }
 
 // ---- x passes through TMA-staged tiles -----------------------------------------------------------
-// Same pipeline as the y pass: persistent CTAs, two buffers, one tile (LPB complex lines = 2 LPB
-// real rows) loading by cp.async.bulk.tensor while the previous one is transformed in place.  A
-// row arrives as xbox_n boxes of xbox_w 8-byte elements, so the staged rows are dense: real rows
-// of nx values going forward, spectrum rows of lx complex values going back.
+// Persistent CTAs walk tiles of LPB complex lines (2 LPB real rows).  A tile's rows arrive by
+// cp.async.bulk.tensor in a ring of stage buffers (xbox_n boxes of xbox_w 8-byte elements per row,
+// so the staged rows are dense: real rows of nx values going forward, spectrum rows of lx complex
+// values going back); pass 0 reads the stage buffer and writes a separate skewed work buffer, after
+// which the stage is refilled with the tile STG strides ahead, so that up to STG tiles are loading
+// while one is transformed.  Two CTAs share an SM.
 template <int N, class C>
 struct XTmaGeom {
 	static constexpr int R = ct_radix(N);
 	static constexpr int LPB = ct_lpb(N, sizeof(C));
 	static constexpr int THREADS = LPB * (N / R);
 	static constexpr size_t WORK = (size_t)SmRows<N, LPB, 4>::SIZE * sizeof(C);
-	// staged rows (at most 2 LPB spectrum rows of N/2 + 1 + padding complex values) fit in WORK
-	// with room to spare for N >= 64; shorter rows use the non-staged kernels
 	static constexpr size_t BUF = (WORK + 127) / 128 * 128;
-	// + the forward pass's Ms table and its twiddle table W_N^k (read once per persistent CTA, so
-	// that its butterflies' twiddles come from shared memory; the inverse pass reads them from
-	// global memory, which measured slightly faster there)
-	static constexpr size_t TW = 2 * BUF + 16 + 256 * (sizeof(C) / 2);
-	static constexpr size_t SMEM = TW + (size_t)N * sizeof(C);
-	static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;
+	static constexpr size_t PER_SM = 228 * 1024;  // shared memory per SM (1 KB of it reserved per CTA)
+	// forward stage: 2 LPB real rows of at most N/2 values and their region bytes
+	static constexpr size_t SB_F = ((size_t)LPB * N * (sizeof(C) / 2 + 1) + 127) / 128 * 128;
+	// forward extras: barriers, the 256-entry Ms table, the twiddle table W_N^k
+	static constexpr size_t EXTRA_F = 64 + 256 * (sizeof(C) / 2) + (size_t)N * sizeof(C);
+	static constexpr int STG_F = 2 * (3 * SB_F + BUF + EXTRA_F + 1024) <= PER_SM ? 3 : 2;
+	static constexpr size_t SMEM_F = STG_F * SB_F + BUF + EXTRA_F;
+	static constexpr int MINB_F = 2 * (SMEM_F + 1024) <= PER_SM ? 2 : 1;
+	// inverse stage: 2 LPB spectrum rows of lx complex values (lx * sizeof(C) * 2 LPB <= BUF,
+	// checked at set-up); the inverse reads its twiddles from global memory
+	static constexpr size_t SB_I = BUF;
+	static constexpr int STG_I = 2 * (3 * SB_I + BUF + 64 + 1024) <= PER_SM ? 3 : 2;
+	static constexpr size_t SMEM_I = STG_I * SB_I + BUF + 64;
+	static constexpr int MINB_I = 2 * (SMEM_I + 1024) <= PER_SM ? 2 : 1;
 };
 
+// After a bounded wait gave up in a ring of STG stage buffers on the tile t of local index k:
+// waits (bounded again) for every load still in flight (tiles t, t + G, ..., t + (STG - 1) G
+// that exist), so that no copy lands in shared memory after the CTA has exited.
+template <int STG>
+__device__ __forceinline__ void mbar_drain_ring(uint64_t *bar, uint32_t parity, int k, int t, int G, int ntiles)
+{
+	for (int i = 0; i < STG; ++i) {
+		const int s = (k + i) % STG;
+		if (t + i * G < ntiles) mbar_wait(&bar[s], (parity >> s) & 1u);
+	}
+}
+
 // Forward: with SCALE the tile's region bytes (rows r % (ny nz), contiguous within a tile) ride
-// along in the same buffer behind the real rows, and the 256-entry Ms table sits in shared memory,
+// along in the same stage behind the real rows, and the 256-entry Ms table sits in shared memory,
 // so that pass 0 reads nothing but shared memory.
 template <typename T, int N, bool SCALE>
-__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB)
+__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB_F)
     k_x_fwd_tma(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ CUtensorMap rmap,
                 const T *__restrict__ ms_tab, cplx<T> *__restrict__ S, int nx, int ny, int nz, int py, int hx,
                 int lx, int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
 	using C = cplx<T>;
 	using G = XTmaGeom<N, C>;
-	constexpr int LPB = G::LPB, TPL = N / G::R;
+	constexpr int LPB = G::LPB, TPL = N / G::R, STG = G::STG_F;
 	using SI = SmRows<N, LPB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
-	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
-	T *msr = reinterpret_cast<T *>(smem_tma + 2 * G::BUF + 16);
+	C *work = reinterpret_cast<C *>(smem_tma + STG * G::SB_F);
+	unsigned char *extra = smem_tma + STG * G::SB_F + G::BUF;
+	uint64_t *bar = reinterpret_cast<uint64_t *>(extra);
+	T *msr = reinterpret_cast<T *>(extra + 64);
+	C *tws = reinterpret_cast<C *>(extra + 64 + 256 * sizeof(T));
 	const int tid = threadIdx.x;
 	const int line = tid / TPL, j0 = tid % TPL;
 	const int rows = 3 * ny * nz, nyz = ny * nz;
+	const int G_ = (int)gridDim.x;
 	const uint32_t row_bytes = (uint32_t)(2 * LPB * (size_t)nx * sizeof(T));
 	const uint32_t tile_bytes = row_bytes + (SCALE ? (uint32_t)(2 * LPB * nx) : 0u);
-	auto issue = [&](int t, int b) {
-		mbar_expect_tx(&bar[b], tile_bytes);
-		tma_load_3d(smem_tma + b * G::BUF, &tmap, 0, 0, t * 2 * LPB, &bar[b]);
-		if (SCALE) tma_load_2d(smem_tma + b * G::BUF + row_bytes, &rmap, 0, (t * 2 * LPB) % nyz, &bar[b]);
+	auto issue = [&](int t, int s) {
+		unsigned char *dst = smem_tma + s * G::SB_F;
+		mbar_expect_tx(&bar[s], tile_bytes);
+		tma_load_3d(dst, &tmap, 0, 0, t * 2 * LPB, &bar[s]);
+		if (SCALE) tma_load_2d(dst + row_bytes, &rmap, 0, (t * 2 * LPB) % nyz, &bar[s]);
 	};
 	if (SCALE)
 		for (int r = tid; r < 256; r += blockDim.x) msr[r] = ms_tab[r];
-	C *tws = reinterpret_cast<C *>(smem_tma + G::TW);
 	for (int q = tid; q < N; q += blockDim.x) tws[q] = twN[q];
 	if (tid == 0) {
-		mbar_init(&bar[0], 1);
-		mbar_init(&bar[1], 1);
+		for (int s = 0; s < STG; ++s) mbar_init(&bar[s], 1);
 		fence_proxy_async();
 	}
 	__syncthreads();
-	if (tid == 0) {
-		if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-		if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
-	}
-	uint32_t parity = 0;
-	int k = 0;
-	for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
-		const int b = k & 1;
-		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+	if (tid == 0)
+		for (int s = 0; s < STG; ++s)
+			if ((int)blockIdx.x + s * G_ < ntiles) issue(blockIdx.x + s * G_, s);
+	uint32_t parity = 0;  // bit s: phase parity expected next on bar[s]
+	int k = 0, s = 0;
+	for (int t = blockIdx.x; t < ntiles; t += G_, ++k, s = s + 1 == STG ? 0 : s + 1) {
+		// (this barrier also orders the previous tile's reads of the work buffer before pass 0)
+		const bool late = !mbar_wait(&bar[s], (parity >> s) & 1u);
 		if (__syncthreads_or(late)) {
 			if (tid == 0) {
 				atomicExch(err, 1);
-				mbar_drain2(bar, parity, b, t + (int)gridDim.x < ntiles);
+				mbar_drain_ring<STG>(bar, parity, k, t, G_, ntiles);
 			}
 			return;
 		}
-		parity ^= 1u << b;
-		C *sm = reinterpret_cast<C *>(smem_tma + b * G::BUF);
-		const T *rowa = reinterpret_cast<const T *>(sm) + (size_t)(2 * line) * nx;
+		parity ^= 1u << s;
+		const unsigned char *stage = smem_tma + s * G::SB_F;
+		const T *rowa = reinterpret_cast<const T *>(stage) + (size_t)(2 * line) * nx;
 		const T *rowb = rowa + nx;
-		const uint8_t *rga = smem_tma + b * G::BUF + row_bytes + (size_t)(2 * line) * nx;
+		const uint8_t *rga = stage + row_bytes + (size_t)(2 * line) * nx;
 		const uint8_t *rgb = rga + nx;
 		const int ra = 2 * (t * LPB + line), rb = ra + 1;
 		const bool va = ra < rows, vb = rb < rows;
@@ -897,70 +919,74 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 			}
 			return C{a, bb};
 		};
-		auto st = [&](int l, int kk, C v) { sm[SI::at(l, kk)] = v; };
-		cta_fft_h0<T, N, G::R, LPB, SI, true>(sm, tws, line, j0, ld, st);  // x >= nx, N/2 <= x: zero
+		auto st = [&](int l, int kk, C v) { work[SI::at(l, kk)] = v; };
+		const int next = t + STG * G_;
+		auto release = [&]() {
+			__syncthreads();  // every thread has read stage s
+			if (tid == 0 && next < ntiles) {
+				fence_proxy_async();
+				issue(next, s);
+			}
+		};
+		cta_fft_h0<T, N, G::R, LPB, SI>(work, tws, line, j0, ld, st, release);  // x >= nx, N/2 <= x: zero
 		__syncthreads();
 		C *Sa = S + ((size_t)(qa / nyz * nz + qa % nyz / ny) * py + qa % nyz % ny) * lx;
 		C *Sb = S + ((size_t)(qb / nyz * nz + qb % nyz / ny) * py + qb % nyz % ny) * lx;
 		const T h = T(0.5);
 		for (int kk = j0; kk < hx; kk += TPL) {
-			const C zk = sm[SI::at(line, kk)], zn = sm[SI::at(line, (N - kk) & (N - 1))];
+			const C zk = work[SI::at(line, kk)], zn = work[SI::at(line, (N - kk) & (N - 1))];
 			if (va) Sa[kk] = C{h * (zk.x + zn.x), h * (zk.y - zn.y)};
 			if (vb) Sb[kk] = C{h * (zk.y + zn.y), h * (zn.x - zk.x)};
 		}
-		const int next = t + 2 * (int)gridDim.x;
-		fence_proxy_async();
-		__syncthreads();
-		if (tid == 0 && next < ntiles) issue(next, b);
 	}
 }
 
 // x inverse: the 2 LPB spectrum rows of a tile lie in one (component, z) plane (ny a multiple of
 // 2 LPB); the 4-D tensor map addresses them as (box element, box, y, plane).
 template <typename T, int N>
-__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB)
+__global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cplx<T>>::MINB_I)
     k_x_inv_tma(const __grid_constant__ CUtensorMap tmap, T *__restrict__ H, int nx, int ny, int hx, int lx,
                 int ntiles, const cplx<T> *__restrict__ twN, int *err)
 {
 	using C = cplx<T>;
 	using G = XTmaGeom<N, C>;
-	constexpr int LPB = G::LPB, TPL = N / G::R;
+	constexpr int LPB = G::LPB, TPL = N / G::R, STG = G::STG_I;
 	using SI = SmRows<N, LPB, 4>;
 	extern __shared__ __align__(128) unsigned char smem_tma[];
-	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + 2 * G::BUF);
+	C *work = reinterpret_cast<C *>(smem_tma + STG * G::SB_I);
+	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_tma + STG * G::SB_I + G::BUF);
 	const int tid = threadIdx.x;
 	const int line = tid / TPL, j0 = tid % TPL;
+	const int G_ = (int)gridDim.x;
 	const uint32_t tile_bytes = (uint32_t)(2 * LPB * (size_t)lx * sizeof(C));
-	auto issue = [&](int t, int b) {
+	auto issue = [&](int t, int s) {
 		const int row0 = t * 2 * LPB;
-		mbar_expect_tx(&bar[b], tile_bytes);
-		tma_load_4d(smem_tma + b * G::BUF, &tmap, 0, 0, row0 % ny, row0 / ny, &bar[b]);
+		mbar_expect_tx(&bar[s], tile_bytes);
+		tma_load_4d(smem_tma + s * G::SB_I, &tmap, 0, 0, row0 % ny, row0 / ny, &bar[s]);
 	};
 	if (tid == 0) {
-		mbar_init(&bar[0], 1);
-		mbar_init(&bar[1], 1);
+		for (int s = 0; s < STG; ++s) mbar_init(&bar[s], 1);
 		fence_proxy_async();
 	}
 	__syncthreads();
-	if (tid == 0) {
-		if ((int)blockIdx.x < ntiles) issue(blockIdx.x, 0);
-		if ((int)(blockIdx.x + gridDim.x) < ntiles) issue(blockIdx.x + gridDim.x, 1);
-	}
+	if (tid == 0)
+		for (int s = 0; s < STG; ++s)
+			if ((int)blockIdx.x + s * G_ < ntiles) issue(blockIdx.x + s * G_, s);
 	uint32_t parity = 0;
-	int k = 0;
-	for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++k) {
-		const int b = k & 1;
-		const bool late = !mbar_wait(&bar[b], (parity >> b) & 1u);
+	int k = 0, s = 0;
+	for (int t = blockIdx.x; t < ntiles; t += G_, ++k, s = s + 1 == STG ? 0 : s + 1) {
+		// (this barrier also orders the previous tile's last-pass reads of the work buffer before
+		// this tile's pass 0 writes)
+		const bool late = !mbar_wait(&bar[s], (parity >> s) & 1u);
 		if (__syncthreads_or(late)) {
 			if (tid == 0) {
 				atomicExch(err, 1);
-				mbar_drain2(bar, parity, b, t + (int)gridDim.x < ntiles);
+				mbar_drain_ring<STG>(bar, parity, k, t, G_, ntiles);
 			}
 			return;
 		}
-		parity ^= 1u << b;
-		C *sm = reinterpret_cast<C *>(smem_tma + b * G::BUF);
-		const C *Sa = sm + (size_t)(2 * line) * lx;
+		parity ^= 1u << s;
+		const C *Sa = reinterpret_cast<const C *>(smem_tma + s * G::SB_I) + (size_t)(2 * line) * lx;
 		const C *Sb = Sa + lx;
 		const size_t ra = 2 * ((size_t)t * LPB + line);
 		T *Ha = H + ra * nx, *Hb = Ha + nx;
@@ -978,11 +1004,15 @@ __global__ void __launch_bounds__(XTmaGeom<N, cplx<T>>::THREADS, XTmaGeom<N, cpl
 				Hb[x] = v.y;
 			}
 		};
-		cta_fft<T, N, G::R, LPB, true, SI, true>(sm, twN, line, j0, ld, st);
-		const int next = t + 2 * (int)gridDim.x;
-		fence_proxy_async();
-		__syncthreads();
-		if (tid == 0 && next < ntiles) issue(next, b);
+		const int next = t + STG * G_;
+		auto release = [&]() {
+			__syncthreads();  // every thread has read stage s
+			if (tid == 0 && next < ntiles) {
+				fence_proxy_async();
+				issue(next, s);
+			}
+		};
+		cta_fft<T, N, G::R, LPB, true, SI>(work, twN, line, j0, ld, st, release);
 	}
 }
 
@@ -1066,18 +1096,18 @@ mm_status fs_setup_x_tma(ConvPlan *p)
 	constexpr int LPB = G::LPB;
 	p->tma_xf = p->tma_xi = false;
 	// the forward pass's half-zero first butterflies need nx <= N/2 (non-periodic zero padding)
-	if (G::SMEM > 227 * 1024 || N < 64 || 2 * p->nx > N) return MM_OK;
+	if (G::SMEM_F > 227 * 1024 || G::SMEM_I > 227 * 1024 || N < 64 || 2 * p->nx > N) return MM_OK;
 	int occ = 0;
 	// forward: dense real rows split into boxes of even width
 	const size_t wf = (size_t)p->nx * sizeof(T) / 8;
 	const size_t nbf = (wf + 255) / 256;
-	if ((p->nx * sizeof(T)) % 16 == 0 && wf % (2 * nbf) == 0 && 2 * LPB * p->nx * sizeof(T) <= G::BUF) {
+	if ((p->nx * sizeof(T)) % 16 == 0 && wf % (2 * nbf) == 0 && 2 * LPB * p->nx * sizeof(T) <= G::SB_F) {
 		// region bytes ride behind the rows when a tile's rows are contiguous in the region map
 		p->tma_xf_scale = p->nx % 16 == 0 && (p->ny * p->nz) % (2 * LPB) == 0 && p->nx / 8 <= 256 &&
-		                  2 * LPB * p->nx * (sizeof(T) + 1) <= G::BUF;
-		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, false>, G::SMEM));
-		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, true>, G::SMEM));
-		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_fwd_tma<T, N, true>, G::THREADS, G::SMEM));
+		                  2 * LPB * p->nx * (sizeof(T) + 1) <= G::SB_F;
+		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, false>, G::SMEM_F));
+		MM_TRY(set_smem<T>((const void *)k_x_fwd_tma<T, N, true>, G::SMEM_F));
+		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_fwd_tma<T, N, true>, G::THREADS, G::SMEM_F));
 		if (occ >= 1) {
 			p->grid_xf = occ * num_sms();
 			p->xf_box_n = (int)nbf;
@@ -1086,14 +1116,14 @@ mm_status fs_setup_x_tma(ConvPlan *p)
 		}
 	}
 	// inverse: spectrum rows of a tile within one plane
-	if (p->ny % (2 * LPB) == 0 && (size_t)2 * LPB * p->lx * sizeof(C) <= G::BUF) {
+	if (p->ny % (2 * LPB) == 0 && (size_t)2 * LPB * p->lx * sizeof(C) <= G::SB_I) {
 		const uint64_t rowb = (uint64_t)p->lx * sizeof(C);
 		const uint64_t dims[4] = {(uint64_t)p->xbox_w, (uint64_t)p->xbox_n, (uint64_t)p->ny, 3ull * p->nz};
 		const uint64_t strides[3] = {(uint64_t)p->xbox_w * 8, rowb, rowb * p->py};
 		const uint32_t box[4] = {(uint32_t)p->xbox_w, (uint32_t)p->xbox_n, (uint32_t)(2 * LPB), 1};
 		MM_TRY(tma_encode(&p->tm_xi, p->spec, 4, dims, strides, box));
-		MM_TRY(set_smem<T>((const void *)k_x_inv_tma<T, N>, G::SMEM));
-		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_inv_tma<T, N>, G::THREADS, G::SMEM));
+		MM_TRY(set_smem<T>((const void *)k_x_inv_tma<T, N>, G::SMEM_I));
+		MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_x_inv_tma<T, N>, G::THREADS, G::SMEM_I));
 		if (occ >= 1) {
 			p->grid_xi = occ * num_sms();
 			p->tma_xi = true;
@@ -1160,11 +1190,11 @@ bool fs_x_fwd_tma(ConvPlan *p, const T *M, const uint8_t *reg, const T *ms_tab, 
 	const int ntiles = (lines + G::LPB - 1) / G::LPB;
 	const int grid = std::min(ntiles, p->grid_xf);
 	if (ms_tab)
-		k_x_fwd_tma<T, N, true><<<grid, G::THREADS, G::SMEM, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
+		k_x_fwd_tma<T, N, true><<<grid, G::THREADS, G::SMEM_F, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
 		                                                            p->nz, p->py, p->hx, p->lx, ntiles,
 		                                                            (const C *)p->tw_x, p->err);
 	else
-		k_x_fwd_tma<T, N, false><<<grid, G::THREADS, G::SMEM, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
+		k_x_fwd_tma<T, N, false><<<grid, G::THREADS, G::SMEM_F, st>>>(*map, *rmap, ms_tab, (C *)p->spec, p->nx, p->ny,
 		                                                             p->nz, p->py, p->hx, p->lx, ntiles,
 		                                                             (const C *)p->tw_x, p->err);
 	return true;
@@ -1177,7 +1207,7 @@ void fs_x_inv_tma(ConvPlan *p, T *H, cudaStream_t st)
 	using G = XTmaGeom<N, C>;
 	const int ntiles = 3 * p->ny * p->nz / (2 * G::LPB);
 	const int grid = std::min(ntiles, p->grid_xi);
-	k_x_inv_tma<T, N><<<grid, G::THREADS, G::SMEM, st>>>(p->tm_xi, H, p->nx, p->ny, p->hx, p->lx, ntiles,
+	k_x_inv_tma<T, N><<<grid, G::THREADS, G::SMEM_I, st>>>(p->tm_xi, H, p->nx, p->ny, p->hx, p->lx, ntiles,
 	                                                     (const C *)p->tw_x, p->err);
 }
 
@@ -1657,8 +1687,8 @@ struct GDesc {
 	const T *tensor;
 	const T *tensor_t;  // fused y+z members: the reduced tensor kx-major, [hx][qz][qy][6]
 	const cplx<T> *tw_x, *tw_y;
-	const T *M[3];
-	T *H;
+	const T *M[4];
+	T *H[2];
 	const uint8_t *reg;
 	const T *ms_tab;
 	const int *flags;   // the member's run flags: [0] runs, [1] gated runs (NULL: always)
@@ -1681,7 +1711,7 @@ __host__ __device__ constexpr int var_lpb(int n, int csize, int v)
 
 __device__ __forceinline__ bool member_skips(const int *flags, int gate)
 {
-	return flags && (!flags[0] || (gate && !flags[1]));
+	return flags && (!flags[0] || (gate && !flags[gate]));
 }
 
 template <typename T, int N, int LPB, int R>
@@ -1698,12 +1728,13 @@ __global__ void __launch_bounds__(LPB * (N / R)) k_x_fwd_grp(const GDesc<T> *__r
 
 template <typename T, int N, int LPB, int R>
 __global__ void __launch_bounds__(LPB * (N / R)) k_x_inv_grp(const GDesc<T> *__restrict__ d,
-                                                                      const int2 *__restrict__ items, int gate)
+                                                                      const int2 *__restrict__ items, int output,
+                                                                      int gate)
 {
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> g = d[it.x];
-	x_inv_ct_body<T, N, LPB, R>(g.spec, g.H, g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
+	x_inv_ct_body<T, N, LPB, R>(g.spec, g.H[output], g.nx, g.ny, g.nz, g.py, g.hx, g.lx, g.tw_x, it.y);
 }
 
 template <typename T, int N, int TB, bool INV, int R>
@@ -2017,6 +2048,7 @@ struct ConvGroup {
 	CUtensorMap *maps = nullptr;  // [2 member + inverse]: spectrum views of the y passes
 	bool maps_ok = false;         // every member's maps exist (variant 3 possible)
 	int *err = nullptr;           // set when a staged pass gave up waiting
+	bool one_output = false;      // some member has no second output
 	std::vector<void *> owned;    // kx-major tensors of the fused members
 	// the lists of one phase (independent members) run side by side on these streams
 	static constexpr int POOL = 8;
@@ -2226,7 +2258,7 @@ mm_status group_smem(int pass, int len, int v)
 
 template <typename T>
 void group_launch_v(const ConvGroup *g, int pass, int len, int v, const int2 *items, int n, int grid, int input,
-                    int gate, cudaStream_t st)
+                    int output, int gate, cudaStream_t st)
 {
 	using C = cplx<T>;
 	const GDesc<T> *d = (const GDesc<T> *)g->desc;
@@ -2267,16 +2299,16 @@ void group_launch_v(const ConvGroup *g, int pass, int len, int v, const int2 *it
 		constexpr int LPB = var_lpb(N, sizeof(C), V), TB = var_tb(N, sizeof(C), V), R = var_radix(N, V);
 		constexpr int TPL = N / R;
 		if (pass == 0) k_x_fwd_grp<T, N, LPB, R><<<n, LPB * TPL, sm, st>>>(d, items, input, gate);
-		if (pass == 4) k_x_inv_grp<T, N, LPB, R><<<n, LPB * TPL, sm, st>>>(d, items, gate);
+		if (pass == 4) k_x_inv_grp<T, N, LPB, R><<<n, LPB * TPL, sm, st>>>(d, items, output, gate);
 		if (pass == 1) k_y_grp<T, N, TB, false, R><<<n, TB * TPL, sm, st>>>(d, items, gate);
 		if (pass == 3) k_y_grp<T, N, TB, true, R><<<n, TB * TPL, sm, st>>>(d, items, gate);
 	});
 }
 
 template <typename T>
-void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, int gate, cudaStream_t st)
+void group_launch(const ConvGroup *g, const ConvGroup::List &l, int input, int output, int gate, cudaStream_t st)
 {
-	group_launch_v<T>(g, l.pass, l.len, l.variant, l.items, l.n, l.grid, input, gate, st);
+	group_launch_v<T>(g, l.pass, l.len, l.variant, l.items, l.n, l.grid, input, output, gate, st);
 }
 
 // Persistent grid of the TMA-staged grouped y pass (resident CTAs on the whole device).
@@ -2339,9 +2371,9 @@ mm_status group_tune(const ConvGroup *g, const ConvGroupMember *m, const std::ve
 		                                                cudaMemcpyHostToDevice, st), "cudaMemcpyAsync");
 		if (r == MM_OK) r = group_smem<T>(pass, len, v);
 		if (r == MM_OK) {
-			group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, st);  // warm-up
+			group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, 0, st);  // warm-up
 			cudaEventRecord(e0, st);
-			for (int k = 0; k < 3; ++k) group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, st);
+			for (int k = 0; k < 3; ++k) group_launch_v<T>(g, pass, len, v, di, (int)items.size(), grid, 0, 0, 0, st);
 			cudaEventRecord(e1, st);
 			r = cuda_status(cudaEventSynchronize(e1), "autotune launch");
 		}
@@ -2374,12 +2406,13 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		d.tensor = (const T *)p->tensor;
 		d.tw_x = (const cplx<T> *)p->tw_x;
 		d.tw_y = (const cplx<T> *)p->tw_y;
-		for (int k = 0; k < 3; ++k) d.M[k] = (const T *)m[i].M[k];
-		d.H = (T *)m[i].H;
+		for (int k = 0; k < 4; ++k) d.M[k] = (const T *)m[i].M[k];
+		for (int k = 0; k < 2; ++k) d.H[k] = (T *)m[i].H[k];
+		if (!d.H[1]) g->one_output = true;
 		d.reg = m[i].reg;
 		d.ms_tab = (const T *)m[i].ms_tab;
 		d.flags = nullptr;  // the autotuner runs every member; the real flags are set below
-		if (!d.reg || !d.ms_tab || !d.H) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
+		if (!d.reg || !d.ms_tab || !d.H[0]) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: member without regions or output");
 		d.nx = p->nx; d.ny = p->ny; d.nz = p->nz; d.py = p->py; d.hx = p->hx; d.lx = p->lx; d.qy = p->qy; d.qz = p->qz;
 		d.tensor_t = nullptr;
 		lists[{0, p->px}].push_back(i);
@@ -2497,9 +2530,11 @@ mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int
 // The lists of one phase (x forward; y forward and fused y+z; z; y inverse; x inverse) touch
 // disjoint members, so each phase forks onto the group's stream pool and joins back on `st`
 // (inside a stream capture this becomes parallel graph branches).
-mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st)
+mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st, int output)
 {
-	if (!g || input < 0 || input > 2) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad input selector");
+	if (!g || input < 0 || input > 3) return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad input selector");
+	if (output < 0 || output > 1 || (output == 1 && g->one_output))
+		return fail(MM_ERR_INVALID_ARGUMENT, "conv group: bad output selector");
 	auto rank = [](int pass) { return pass == 6 ? 1 : pass; };
 	size_t i = 0;
 	while (i < g->lists.size()) {
@@ -2507,8 +2542,8 @@ mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st)
 		while (j < g->lists.size() && rank(g->lists[j].pass) == rank(g->lists[i].pass)) ++j;
 		const int n = (int)(j - i);
 		if (n == 1) {
-			if (g->prec == MM_F64) group_launch<double>(g, g->lists[i], input, gate, st);
-			else group_launch<float>(g, g->lists[i], input, gate, st);
+			if (g->prec == MM_F64) group_launch<double>(g, g->lists[i], input, output, gate, st);
+			else group_launch<float>(g, g->lists[i], input, output, gate, st);
 			MM_TRY(after_launch("k_conv_grp"));
 		} else {
 			MM_CUDA(cudaEventRecord(g->fork, st));
@@ -2516,8 +2551,8 @@ mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st)
 			for (int q = 0; q < used; ++q) MM_CUDA(cudaStreamWaitEvent(g->pool[q], g->fork, 0));
 			for (size_t k = i; k < j; ++k) {
 				cudaStream_t sq = g->pool[(k - i) % ConvGroup::POOL];
-				if (g->prec == MM_F64) group_launch<double>(g, g->lists[k], input, gate, sq);
-				else group_launch<float>(g, g->lists[k], input, gate, sq);
+				if (g->prec == MM_F64) group_launch<double>(g, g->lists[k], input, output, gate, sq);
+				else group_launch<float>(g, g->lists[k], input, output, gate, sq);
 				MM_TRY(after_launch("k_conv_grp"));
 			}
 			for (int q = 0; q < used; ++q) {

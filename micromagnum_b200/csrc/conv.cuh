@@ -63,20 +63,20 @@ int conv_launches(const ConvPlan *p);
 
 // Grouped convolution over many plans of the same precision, each with power-of-two 3-D padding
 // and a register z pass: one launch per pass and transform length covers every member.  M[k]
-// are up to three candidate inputs per member (selected per call), H its output; flags (device,
-// optional) are the member's run flags: flags[0] == 0 skips it, and with gate != 0 so does
-// flags[1] == 0.
+// are up to four candidate inputs per member and H[k] up to two outputs (each selected per call;
+// H[1] may be NULL, then only output 0 is allowed); flags (device, optional) are the member's run
+// flags: flags[0] == 0 skips it, and with gate != 0 so does flags[gate] == 0.
 struct ConvGroup;
 struct ConvGroupMember {
 	ConvPlan *plan;
-	const void *M[3];
-	void *H;
+	const void *M[4];
+	void *H[2];
 	const uint8_t *reg;
 	const void *ms_tab;  // 256 entries
 	const int *flags;    // device run flags, NULL: always run
 };
 mm_status conv_group_create(ConvGroup **out, const ConvGroupMember *members, int count, cudaStream_t st);
-mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st);
+mm_status conv_group_execute(ConvGroup *g, int input, int gate, cudaStream_t st, int output = 0);
 int conv_group_launches(const ConvGroup *g);
 void conv_group_destroy(ConvGroup *g);
 // Whether a member with these padded lengths takes the grouped fused y+z pass (which keeps a

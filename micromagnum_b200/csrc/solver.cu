@@ -386,19 +386,76 @@ constexpr int STAGE_PRE = 6 + 3 * (MAXS - 1);
 template <typename T>
 constexpr size_t stage_smem() { return (size_t)STAGE_PRE * STAGE_CPT * 256 * sizeof(T); }
 
+// Deviation form of the FP32 batched stages.  The state is y = hi + D with hi the instance's base
+// state (fixed between rebases) and D its deviation (small); the base field hb = H_demag(hi) +
+// H_exch(hi) is computed once per rebase.  A stage input y_l = hi + D_l is carried as D_l alone, its
+// demag field is the convolution of D_l, and the right-hand side is split into a base part built
+// from hi and hb + H_zeeman only (bit-identical in every stage of a step while the applied field is
+// constant) and a part built from D_l and the fields of D_l:
+//   H = Hb + dH,  Hb = hb + H_z(t),  dH = H_demag(D) + H_exch(D)
+//   y x H = hi x Hb + [hi x dH + D x (Hb + dH)] = Tb + dT
+//   y x (y x H) = hi x Tb + [hi x dT + D x (Tb + dT)] = Ub + dU
+//   dm/dt = (l1 Tb + l2 Ub) + (l1 dT + l2 dU)
+// Rounding in a stage then differs from the other stages of the step only in proportion to the
+// deviation terms, so the embedded error estimate keeps no floor of order float epsilon times the
+// field: a direct FP32 evaluation of y_l has one (~1e-4 relative to h max |dm/dt| near equilibrium
+// for 4 nm cells), at which the controller's relative test stalls the step size.  Terms: demag,
+// exchange and the applied field (the batched instances' physics).
+template <typename T>
+__device__ __forceinline__ bool cell_rhs_delta(const CellArgs<T> &a, const T *__restrict__ msr,
+                                               const T *__restrict__ D, size_t n, int x, int yy, int z, size_t i,
+                                               V3<T> hi, V3<T> hb, V3<T> hdD, double t, V3<T> &Tt, V3<T> &dm)
+{
+	const DevMat<T> &M = mat_of(a, i);
+	const V3<T> Hz = zeeman_field(a, t);
+	if (M.Ms == T(0)) {
+		Tt = v3<T>(0, 0, 0);
+		dm = v3<T>(0, 0, 0);
+		return false;
+	}
+	const V3<T> d = load3(D, i, n);
+	V3<T> dH = (a.terms & MM_TERM_DEMAG) ? hdD : v3<T>(0, 0, 0);
+	if (a.terms & MM_TERM_EXCHANGE) {
+		bool has[6];
+		size_t off[6];
+		neighbours(a, x, yy, z, i, has, off);
+		const T w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
+		V3<T> sum = v3<T>(0, 0, 0);
+#pragma unroll
+		for (int q = 0; q < 6; ++q) {
+			if (!has[q]) continue;
+			const T ms_q = a.reg ? msr[a.reg[off[q]]] : M.Ms;
+			if (ms_q != T(0)) sum = sum + w[q] * (load3(D, off[q], n) - d);
+		}
+		dH = dH + M.cex * sum;
+	}
+	const V3<T> Hb = hb + Hz;
+	const V3<T> Tb = cross(hi, Hb);
+	const V3<T> dT = cross(hi, dH) + cross(d, Hb + dH);
+	Tt = Tb + dT;
+	const V3<T> Ub = cross(hi, Tb);
+	const V3<T> dU = cross(hi, dT) + cross(d, Tt);
+	dm = (M.l1 * Tb + M.l2 * Ub) + (M.l1 * dT + M.l2 * dU);
+	return true;
+}
+
 // One tile (32*STAGE_CPT x 8 cells of plane z) of the fused stage; the maxima of the error, of
 // |k_0| and (TORQUE) of |m x H_eff| / Ms accumulate in e2, k02, tq2.  The operands of the stage
 // combination (y_n, its compensation, the earlier stage vectors with nonzero weight) are copied
 // into shared memory asynchronously while the field and k_i are computed; `pre` is the block's
 // STAGE_PRE * STAGE_CPT * 256 slots.
-template <typename T, bool COMP, int S, bool TORQUE>
+// DELTA (the FP32 batched form, with COMP): y_in, the combination and y_out are deviations from
+// the base state yhi (ylo: the step's own deviation D_n), hb the base field (cell_rhs_delta), and
+// the last stage writes the deviation of y_{n+1} into y_out alone (y_out_lo is not written).
+template <typename T, bool COMP, int S, bool TORQUE, bool DELTA = false>
 __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__restrict__ msr, const StageCoef &sc,
                                            const T *__restrict__ y_in, const T *__restrict__ Hd,
                                            const T *__restrict__ yhi, const T *__restrict__ ylo, T *const *K,
                                            T *__restrict__ y_out, T *__restrict__ y_out_lo,
                                            const DevState *__restrict__ st, int tile, int tiles_x, int tiles_y,
-                                           T &e2, T &k02, T &tq2, T *pre)
+                                           T &e2, T &k02, T &tq2, T *pre, const T *__restrict__ hb = nullptr)
 {
+	static_assert(!DELTA || COMP, "the deviation form is the compensated FP32 form's");
 	const size_t n = (size_t)a.nx * a.ny * a.nz;
 	const double h = st->h;
 	const int tx = tile % tiles_x, rest = tile / tiles_x;
@@ -424,7 +481,7 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 		if (in[u]) {
 			for (int c = 0; c < 3; ++c) {
 				const size_t e = idx[u] + c * n;
-				if (out) cp_async_elem(&slot(u, c), yhi + e);
+				if (out && !DELTA) cp_async_elem(&slot(u, c), yhi + e);
 				if (out && COMP) cp_async_elem(&slot(u, 3 + c), ylo + e);
 #pragma unroll
 				for (int l = 0; l < S; ++l)
@@ -435,7 +492,16 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 #pragma unroll
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
-		if (in[u]) {
+		if (in[u] && DELTA) {
+			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
+			V3<T> Tt;
+			const bool mat = cell_rhs_delta<T>(a, msr, y_in, n, x, yy, z, idx[u], load3(yhi, idx[u], n),
+			                                   load3(hb, idx[u], n), hd, t, Tt, ki[u]);
+			if (TORQUE && mat) {
+				const T ms = mat_of(a, idx[u]).Ms;
+				tq2 = nan_max(tq2, dot(Tt, Tt) / (ms * ms));
+			}
+		} else if (in[u]) {
 			V3<T> Heff;
 			const V3<T> hd = (a.terms & MM_TERM_DEMAG) ? load3(Hd, idx[u], n) : v3<T>(0, 0, 0);
 			cell_rhs<T>(a, msr, y_in, n, x, yy, z, idx[u], hd, t, Heff, ki[u]);
@@ -462,7 +528,7 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 					if (f != T(0)) acc = acc + f * pre3(u, 6 + 3 * l);
 				}
 				acc = acc + (T)(h * sc.bn[S]) * ki[u];
-				if (COMP) acc = pre3(u, 0) + acc;
+				if (COMP && !DELTA) acc = pre3(u, 0) + acc;
 				store3(y_out, i, n, acc);
 			}
 			if (sc.reduce_k0) {
@@ -483,7 +549,9 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 			}
 			e2 = nan_max(e2, dot(err, err));
 			if (sc.write_new) {
-				if (COMP) {
+				if (DELTA) {
+					store3(y_out, i, n, pre3(u, 3) + acc);  // deviation of y_{n+1} from the base state
+				} else if (COMP) {
 					// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
 					const V3<T> hi = pre3(u, 0);
 					const V3<T> d = pre3(u, 3) + acc;
@@ -2150,12 +2218,15 @@ struct BSlot {
 	BState bs;
 	int active;  // takes part in rounds
 	int need_k0; // the next round evaluates k_0 at the state (after set-up or a new state)
+	int rebase;  // FP32: the next round first moves the deviation into the base state and
+	             // recomputes the base field (after set-up, then every BATCH_REBASE attempts)
 };
 
 template <typename T>
 struct BDesc {
 	CellArgs<T> a;
 	T *m, *m_lo, *ys[2], *hd, *ynew_lo;
+	T *hb;  // FP32 deviation form: the base field H_demag(m) + H_exch(m) (the ynew_lo buffer)
 	KTab<T> *kt;
 	DevState *ds;
 	BSlot *slot;
@@ -2165,6 +2236,9 @@ struct BDesc {
 
 constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage kernel
 constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
+// FP32 batches (deviation form, cell_rhs_delta): attempts between rebases of an instance.  The
+// stage inputs' rounding grows with the deviation accumulated since the last rebase.
+constexpr int BATCH_REBASE = 8;
 
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
 // K0: the k_0 evaluation of instances that need it (others skip it).
@@ -2181,12 +2255,14 @@ __global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
 	if (threadIdx.x == 0 && threadIdx.y == 0) a = g.a;
 	__syncthreads();
 	load_ms_table(a, msr);
-	const T *y_in = in == 0 ? g.m : g.ys[in - 1];
+	// (FP32: the deviation form, whose k_0 input is the deviation D_n itself)
+	const T *y_in = in == 0 ? (COMP ? g.m_lo : g.m) : g.ys[in - 1];
 	T *const *K = g.kt->k;  // read per use (cached), not held in registers
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
 	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
-		stage_tile<T, COMP, S, TORQUE>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds, it.y + k,
-		                               g.tiles_x, g.tiles_y, e2, k02, tq2, reinterpret_cast<T *>(stage_pre));
+		stage_tile<T, COMP, S, TORQUE, COMP>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds,
+		                                     it.y + k, g.tiles_x, g.tiles_y, e2, k02, tq2,
+		                                     reinterpret_cast<T *>(stage_pre), g.hb);
 	if (sc.last) block_max_to(&g.ds->max_err2, e2);
 	if (sc.reduce_k0) block_max_to(&g.ds->max_k02, k02);
 	if (TORQUE) block_max_to(&g.ds->max_tq2, tq2);
@@ -2206,8 +2282,53 @@ __global__ void __launch_bounds__(256) k_prepare1_grp(const BDesc<T> *__restrict
 	const T *k0 = g.kt->k[0];
 	const size_t end = min(n3, (size_t)(it.y + 1) * BATCH_CHUNK);
 	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x) {
-		if (COMP) g.ys[0][i] = g.m[i] + (g.m_lo[i] + f * k0[i]);
+		if (COMP) g.ys[0][i] = g.m_lo[i] + f * k0[i];  // deviation of y_1
 		else g.ys[0][i] = g.m[i] + f * k0[i];
+	}
+}
+
+// FP32 rebase (instances flagged for it): the base state takes the deviation, hi + D = s + e
+// with s = fl(hi + D) and the rounding error e exact (two-sum), so the state is unchanged.
+__global__ void __launch_bounds__(256) k_rebase_grp(const BDesc<float> *__restrict__ d, const int2 *__restrict__ items)
+{
+	const int2 it = items[blockIdx.x];
+	const BDesc<float> &g = d[it.x];
+	if (!g.slot->active || !g.slot->rebase) return;
+	const size_t n3 = 3 * (size_t)g.n;
+	const size_t end = min(n3, (size_t)(it.y + 1) * BATCH_CHUNK);
+	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x) {
+		const float a = g.m[i], b = g.m_lo[i];
+		const float s = a + b;
+		const float bb = s - a;
+		g.m[i] = s;
+		g.m_lo[i] = (a - (s - bb)) + (b - bb);
+	}
+}
+
+// FP32 base field after a rebase: hb holds H_demag(hi) (the grouped convolution's second output);
+// the material cells add H_exch(hi), with the stencil of cell_core (exchange_cpu.cpp:60-139).
+__global__ void __launch_bounds__(256) k_base_grp(const BDesc<float> *__restrict__ d, const int2 *__restrict__ items)
+{
+	const int2 it = items[blockIdx.x];
+	const BDesc<float> &g = d[it.x];
+	if (!g.slot->active || !g.slot->rebase || !(g.a.terms & MM_TERM_EXCHANGE)) return;
+	const CellArgs<float> &a = g.a;
+	const size_t n = (size_t)g.n;
+	const size_t end = min(n, (size_t)(it.y + 1) * BATCH_CHUNK);
+	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x) {
+		const DevMat<float> &M = mat_of(a, i);
+		if (M.Ms == 0.f) continue;
+		const int x = (int)(i % a.nx), yy = (int)(i / a.nx % a.ny), z = (int)(i / ((size_t)a.nx * a.ny));
+		bool has[6];
+		size_t off[6];
+		neighbours(a, x, yy, z, i, has, off);
+		const float w[6] = {a.wx, a.wx, a.wy, a.wy, a.wz, a.wz};
+		const V3<float> m = load3(g.m, i, n);
+		V3<float> sum = v3<float>(0, 0, 0);
+#pragma unroll
+		for (int q = 0; q < 6; ++q)
+			if (has[q] && mat_of(a, off[q]).Ms != 0.f) sum = sum + w[q] * (load3(g.m, off[q], n) - m);
+		store3(g.hb, i, n, load3(g.hb, i, n) + M.cex * sum);
 	}
 }
 
@@ -2222,8 +2343,20 @@ __global__ void __launch_bounds__(256) k_accept_grp(const BDesc<T> *__restrict__
 	const size_t n = (size_t)g.n;
 	const T *ynew = g.ys[last_buf];
 	const size_t end = min(n, (size_t)(it.y + 1) * BATCH_CHUNK);
-	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x)
-		accept_cell<T, COMP>(n, ynew, g.ynew_lo, g.m, g.m_lo, i);
+	for (size_t i = (size_t)it.y * BATCH_CHUNK + threadIdx.x; i < end; i += blockDim.x) {
+		if (COMP) {
+			// deviation form: y_{n+1} = hi + D (in double), normalised; hi stays, D takes the rest
+			double v[3], l2 = 0.0;
+			for (int c = 0; c < 3; ++c) {
+				v[c] = (double)g.m[i + c * n] + (double)ynew[i + c * n];
+				l2 += v[c] * v[c];
+			}
+			const double sc = l2 > 0 ? 1.0 / sqrt(l2) : 0.0;
+			for (int c = 0; c < 3; ++c) g.m_lo[i + c * n] = (T)(v[c] * sc - (double)g.m[i + c * n]);
+		} else {
+			accept_cell<T, COMP>(n, ynew, g.ynew_lo, g.m, g.m_lo, i);
+		}
+	}
 }
 
 // Grouped step controller (one thread per instance): the single-instance controller's decision,
@@ -2251,6 +2384,7 @@ __global__ void k_controller_grp(const BDesc<T> *__restrict__ d, int count, doub
 	BState &b = sl->bs;
 	b.attempts++;
 	sl->need_k0 = 0;
+	sl->rebase = b.attempts % BATCH_REBASE == 0;
 	const double t_end = d[i].t_end;
 	if (st->not_finite) {
 		b.status = 2;
@@ -2293,6 +2427,7 @@ __global__ void k_slot_start(DevState *st, BSlot *sl, double h0, double t_end)
 	sl->bs = BState{0, 0, 0, 0, 0.0, h};
 	sl->active = 1;
 	sl->need_k0 = 1;
+	sl->rebase = 1;
 }
 
 // Stops an instance (its slot keeps its results).
@@ -2399,13 +2534,23 @@ mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 	constexpr bool COMP = sizeof(T) == 4;
 	const Tableau tb = make_tableau(MM_RK_DP54);
 	const BDesc<T> *d = (const BDesc<T> *)b->desc;
+	if constexpr (COMP) {
+		// instances flagged for a rebase: base state, then its field (convolution output 1, gated
+		// by the rebase flag), then its exchange part
+		const BDesc<float> *df = (const BDesc<float> *)b->desc;
+		k_rebase_grp<<<b->n_cell3, 256, 0, st>>>(df, b->cell3_items);
+		MM_TRY(after_launch("k_rebase_grp"));
+		MM_TRY(conv_group_execute(b->conv, 0, 2, st, 1));
+		k_base_grp<<<b->n_cell, 256, 0, st>>>(df, b->cell_items);
+		MM_TRY(after_launch("k_base_grp"));
+	}
 	if (with_k0) {
 		StageCoef sc{};
 		sc.stage = 0;
 		sc.a_i = tb.a[0];
 		sc.write_next = 1;
 		sc.bn[0] = tb.b[1][0];
-		MM_TRY(conv_group_execute(b->conv, 0, 1, st));
+		MM_TRY(conv_group_execute(b->conv, COMP ? 3 : 0, 1, st));
 		MM_TRY((stage_grp<T, COMP>(b, sc, 0, 0, st)));
 	}
 	k_prepare1_grp<T, COMP><<<b->n_cell3, 256, 0, st>>>(d, tb.b[1][0], b->cell3_items);
@@ -2503,6 +2648,7 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 		d.ys[1] = (T *)s->ys[1];
 		d.hd = (T *)s->hd;
 		d.ynew_lo = (T *)s->ynew_lo;
+		d.hb = sizeof(T) == 4 ? (T *)s->ynew_lo : nullptr;
 		d.kt = (KTab<T> *)s->ktab;
 		d.ds = s->dst;
 		d.slot = sl.dev;
@@ -2516,7 +2662,9 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 		for (int t = 0; t < d.ntiles; t += BATCH_TILES) si.push_back(make_int2(i, t));
 		for (int c = 0; (size_t)c * BATCH_CHUNK < 3 * s->n; ++c) c3.push_back(make_int2(i, c));
 		for (int c = 0; (size_t)c * BATCH_CHUNK < s->n; ++c) c1.push_back(make_int2(i, c));
-		mem.push_back(ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1]}, s->hd, s->reg, s->ms_tab, &sl.dev->active});
+		mem.push_back(ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1], s->m_lo},
+		                              {s->hd, sizeof(T) == 4 ? s->ynew_lo : nullptr}, s->reg, s->ms_tab,
+		                              &sl.dev->active});
 	}
 	b->dirty = false;
 	if (b->members.empty()) return MM_OK;

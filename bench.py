@@ -371,6 +371,8 @@ def run_ours(args, rank, world, local_rank):
             "data": "synthetic (seeded grains, axes, initial m)",
             "config": {"workload": WORKLOAD, "cells": n, "rhs_evals": evals, "accepted_steps": steps,
                        "attempts": attempts, "parallelism": f"{world} independent replicas (one slab per GPU)",
+                       "stage_kernel": ["per-thread loads", "staged, run-time terms", "staged, term set",
+                                        "staged, term set and dp54 stage patterns"][s.stats["stage_kernel"]],
                        "l2": "working set ~0.9 GB per step, larger than the 126 MB L2 (no flush needed)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 3 * n * 8, "d2h_bytes_per_step": 3 * n * 8},
             "gpu_launches": launches,
@@ -681,12 +683,13 @@ def main():
     ap.add_argument("--workload", choices=["slab", "batch", "serve"], default="slab",
                     help="slab: the granular slab throughput (default); batch: 256 batched relaxations; "
                          "serve: a served request stream")
-    ap.add_argument("--serve-requests", type=int, default=32)
-    ap.add_argument("--serve-rates", default="50,100,200,500,1000,2000")
+    ap.add_argument("--serve-requests", type=int, default=128,
+                    help="requests per rate (enough to keep the server busy for the whole deadline)")
+    ap.add_argument("--serve-rates", default="50,2000")
     ap.add_argument("--serve-memory-gb", type=float, default=100.0)
     ap.add_argument("--serve-budget", type=float, default=90.0, help="seconds per arrival rate")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
-    ap.add_argument("--batch-rounds", type=int, default=100000)
+    ap.add_argument("--batch-rounds", type=int, default=2000000)
     ap.add_argument("--batch-budget", type=float, default=900.0, help="device seconds for the batched rounds")
     ap.add_argument("--batch-sample", type=int, default=16,
                     help="instances (a seeded sample) solved one at a time in FP64 for the ratio")

@@ -265,6 +265,9 @@ typedef struct {
 	double last_error;     /* e_abs of the last attempt (max |m_err|) */
 	double last_max_dmdt;  /* max |dm/dt| of the last attempt [rad/s] */
 	int not_finite;        /* 1 if a NaN/Inf was seen in the last attempt */
+	int stage_kernel;      /* fused stage kernel in use: 0 per-thread loads, 1 staged (run-time
+	                        * terms), 2 staged for the term set, 3 staged for the term set and the
+	                        * Dormand-Prince stage patterns */
 } mm_solver_stats;
 
 typedef struct mm_solver mm_solver;

@@ -83,7 +83,7 @@ class mm_solver_stats(ctypes.Structure):
         ("t", ctypes.c_double), ("h", ctypes.c_double), ("h_next", ctypes.c_double),
         ("steps", ctypes.c_int64), ("attempts", ctypes.c_int64), ("rejected", ctypes.c_int64),
         ("last_error", ctypes.c_double), ("last_max_dmdt", ctypes.c_double),
-        ("not_finite", ctypes.c_int),
+        ("not_finite", ctypes.c_int), ("stage_kernel", ctypes.c_int),
     ]
 
 

@@ -356,6 +356,65 @@ __host__ __device__ inline int stage_ops(const StageCoef &sc, int S, bool comp, 
 	return n;
 }
 
+// Structure of one stage as a bit pattern: which k_l the combination reads (bits 0-6), last (7),
+// write_next (8), write_new (9), reduce_k0 (10), which b/c weights are nonzero (11-17), which
+// error weights are nonzero (18-24), and bit 25 set.  A staged stage kernel compiled for a
+// pattern folds its operand indices and weight tests at compile time; PAT_RUNTIME reads them
+// from the coefficients.
+constexpr int PAT_RUNTIME = -1;
+constexpr int PAT_KBITS = 7;  // stage vectors a pattern describes (k_0 .. k_6)
+__host__ __device__ constexpr int pat_make(int needk, bool last, bool wnext, bool wnew, bool rk0, int bnm, int ecm)
+{
+	return needk | (last ? 1 << 7 : 0) | (wnext ? 1 << 8 : 0) | (wnew ? 1 << 9 : 0) | (rk0 ? 1 << 10 : 0) |
+	       (bnm << 11) | (ecm << 18) | (1 << 25);
+}
+__host__ __device__ constexpr bool pat_bit(int pat, int bit) { return ((pat >> bit) & 1) != 0; }
+__host__ __device__ constexpr int pat_nops(int pat, bool comp, bool demag)
+{
+	const bool out = pat_bit(pat, 7) ? pat_bit(pat, 9) : pat_bit(pat, 8);
+	int n = (demag ? 1 : 0) + (out ? 1 : 0) + (out && comp ? 1 : 0);
+	for (int q = 0; q < PAT_KBITS; ++q) n += pat_bit(pat, q) ? 1 : 0;
+	return n;
+}
+// operand index of k_l under a pattern (operands: demag field, y_n, its compensation, the k_l read)
+__host__ __device__ constexpr int pat_kop(int pat, bool comp, bool demag, int l)
+{
+	const bool out = pat_bit(pat, 7) ? pat_bit(pat, 9) : pat_bit(pat, 8);
+	int n = (demag ? 1 : 0) + (out ? 1 : 0) + (out && comp ? 1 : 0);
+	for (int q = 0; q < l; ++q) n += pat_bit(pat, q) ? 1 : 0;
+	return pat_bit(pat, l) ? n : -1;
+}
+__host__ inline int pattern_of(const StageCoef &sc, int S)
+{
+	int needk = 0, bnm = 0, ecm = 0;
+	for (int l = 0; l < MAXS; ++l) {
+		const bool k = stage_needs_k(sc, S, l), b = sc.bn[l] != 0.0, e = sc.ec[l] != 0.0;
+		if (l >= PAT_KBITS && (k || b || e)) return PAT_RUNTIME;  // beyond what a pattern holds
+		needk |= k ? 1 << l : 0;
+		bnm |= b ? 1 << l : 0;
+		ecm |= e ? 1 << l : 0;
+	}
+	return pat_make(needk, sc.last, sc.write_next, sc.write_new, sc.reduce_k0, bnm, ecm);
+}
+// The Dormand-Prince 5(4) stages (magnum/evolver/tableaus.py): nonzero masks of b[i][0..i-1]
+// (b[6][1] = 0), of c = b[6] and of the error weights c4 - c5 (zero at l = 1 only).
+constexpr int dp54_bmask(int i) { return i == 6 ? 0x3D : (1 << i) - 1; }
+constexpr int DP54_CMASK = 0x3D, DP54_ECMASK = 0x7D;
+constexpr int dp54_pattern(int S, bool comp)
+{
+	if (S == 0) return pat_make(0, false, true, false, false, dp54_bmask(1), 0);
+	const bool last = S == 6, rk0 = S == 1, wnew = last && comp;
+	const int bnm = last ? DP54_CMASK : dp54_bmask(S + 1);
+	const int ecm = last ? DP54_ECMASK : 0;
+	int needk = 0;
+	for (int l = 0; l < S; ++l) {
+		const bool need = last ? (pat_bit(ecm, l) || (wnew && pat_bit(bnm, l)))
+		                       : (pat_bit(bnm, l) || (rk0 && l == 0));
+		needk |= need ? 1 << l : 0;
+	}
+	return pat_make(needk, last, !last, wnew, rk0, bnm, ecm);
+}
+
 // One fused stage: k_i = f(y_in) (demag field from Hd), then the next stage state
 // y_{i+1} = y_n + h sum_{l<=i} b_{i+1,l} k_l, or on the last stage the error maximum and y_{n+1}.
 // COMP: compensated float state (y_n = yhi + ylo).  S = i is a template argument, so the sums
@@ -640,7 +699,7 @@ inline bool stage_tma_fits(int nx, size_t esize, bool regions)
 	return (nx * esize) % 16 == 0 && (!regions || nx % 16 == 0);
 }
 
-template <typename T, bool COMP, int S, int TM>
+template <typename T, bool COMP, int S, int TM, int PAT = PAT_RUNTIME>
 __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
     k_stage_tma(const __grid_constant__ StageMaps maps, CellArgs<T> a, StageCoef sc, const KTab<T> *__restrict__ ktab,
                 T *__restrict__ y_out, T *__restrict__ y_out_lo, DevState *__restrict__ st, int tiles_x,
@@ -658,6 +717,19 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 	const bool demag = term_on<TM>(a, MM_TERM_DEMAG);
 	int kop[MAXS], op_hd, op_hi, op_lo;
 	const int nops = stage_ops(sc, S, COMP, demag, kop, op_hd, op_hi, op_lo);
+	// the consumers' view of the stage structure: compile-time constants under a pattern (the host
+	// launches a pattern only where it equals the coefficients' own, and only with the demag term)
+	constexpr bool CT = PAT != PAT_RUNTIME;
+	static_assert(!CT || (TM >= 0 && (TM & MM_TERM_DEMAG)), "stage patterns assume a fixed term set with demag");
+	const bool s_last = CT ? pat_bit(PAT, 7) : sc.last != 0;
+	const bool s_wnext = CT ? pat_bit(PAT, 8) : sc.write_next != 0;
+	const bool s_wnew = CT ? pat_bit(PAT, 9) : sc.write_new != 0;
+	const bool s_rk0 = CT ? pat_bit(PAT, 10) : sc.reduce_k0 != 0;
+	constexpr bool CT_OUT = CT && (pat_bit(PAT, 7) ? pat_bit(PAT, 9) : pat_bit(PAT, 8));
+	const int c_hd = CT ? 0 : op_hd, c_hi = CT ? (CT_OUT ? 1 : -1) : op_hi,
+	          c_lo = CT ? (CT_OUT && COMP ? 2 : -1) : op_lo;
+	auto c_kop = [&](int l) -> int { return CT ? pat_kop(PAT, COMP, true, l) : kop[l]; };
+	const int c_nops = CT ? pat_nops(PAT, COMP, true) : nops;
 	// barriers: halo planes arrived [ST_RING], operands arrived [ST_NOB], step done [ST_NOB]
 	uint64_t *bar = reinterpret_cast<uint64_t *>(smem_st + G::YB + G::RB + ST_NOB * (size_t)nops * G::OPB);
 	uint64_t *bar_o = bar + ST_RING, *bar_done = bar + ST_RING + ST_NOB;
@@ -800,7 +872,7 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 					const uint8_t *rz = rs + (gz % ST_RING) * G::RSLOT + rcell;
 					const uint8_t *rm = rs + ((gz + ST_RING - 1) % ST_RING) * G::RSLOT + rcell;
 					const uint8_t *rp = rs + ((gz + 1) % ST_RING) * G::RSLOT + rcell;
-					const T *oc = os + ob * nops * OS + ly * ST_X + lx;
+					const T *oc = os + ob * c_nops * OS + ly * ST_X + lx;
 					auto O3 = [&](int k) -> V3<T> {
 						const T *o = oc + k * OS;
 						return v3<T>(o[0], o[OC], o[2 * OC]);
@@ -808,7 +880,7 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 					auto Y3 = [&](const T *p, int off) -> V3<T> { return v3<T>(p[off], p[off + YC], p[off + 2 * YC]); };
 					const int rg = a.reg ? *rz : 0;
 					const DevMat<T> &M = a.mat[rg < a.nmat ? rg : 0];
-					const V3<T> hd = demag ? O3(op_hd) : v3<T>(0, 0, 0);
+					const V3<T> hd = demag ? O3(c_hd) : v3<T>(0, 0, 0);
 					V3<T> Heff, ki;
 					if (M.Ms == T(0)) {
 						ki = v3<T>(0, 0, 0);
@@ -839,20 +911,20 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 						p[n] = v.y;
 						p[2 * n] = v.z;
 					};
-					if (!sc.last) {
-						if (sc.write_next) {
-							V3<T> acc = COMP ? O3(op_lo) : O3(op_hi);
+					if (!s_last) {
+						if (s_wnext) {
+							V3<T> acc = COMP ? O3(c_lo) : O3(c_hi);
 #pragma unroll
 							for (int l = 0; l < S; ++l) {
 								const T f = fb[l];
-								if (f != T(0)) acc = acc + f * O3(kop[l]);
+								if (CT ? pat_bit(PAT, 11 + l) : f != T(0)) acc = acc + f * O3(c_kop(l));
 							}
 							acc = acc + fb[S] * ki;
-							if (COMP) acc = O3(op_hi) + acc;
+							if (COMP) acc = O3(c_hi) + acc;
 							put3(py, acc);
 						}
-						if (sc.reduce_k0) {
-							const V3<T> k0 = S == 0 ? ki : O3(kop[0]);
+						if (s_rk0) {
+							const V3<T> k0 = S == 0 ? ki : O3(c_kop(0));
 							k02 = max(k02, dot(k0, k0));
 						}
 					} else {
@@ -862,24 +934,26 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 						for (int l = 0; l <= S; ++l) {
 							const T fel = fe[l];
 							const T fc = fb[l];
-							if (fel == T(0) && (!sc.write_new || fc == T(0))) continue;
-							const V3<T> kl = l == S ? ki : O3(kop[l]);
+							if (CT ? (!pat_bit(PAT, 18 + l) && (!s_wnew || !pat_bit(PAT, 11 + l)))
+							       : (fel == T(0) && (!s_wnew || fc == T(0))))
+								continue;
+							const V3<T> kl = l == S ? ki : O3(c_kop(l));
 							err = err + fel * kl;
-							if (sc.write_new) acc = acc + fc * kl;
+							if (s_wnew) acc = acc + fc * kl;
 						}
 						e2 = nan_max(e2, dot(err, err));
-						if (sc.write_new) {
+						if (s_wnew) {
 							if (COMP) {
 								// y_{n+1} = hi + (lo + delta) with an error-free sum: new hi + new lo
-								const V3<T> hi = O3(op_hi);
-								const V3<T> d = O3(op_lo) + acc;
+								const V3<T> hi = O3(c_hi);
+								const V3<T> d = O3(c_lo) + acc;
 								const V3<T> s = hi + d;
 								const V3<T> bb = s - hi;
 								const V3<T> lo = (hi - (s - bb)) + (d - bb);
 								put3(py, s);
 								put3(y_out_lo + i, lo);
 							} else {
-								put3(py, O3(op_hi) + acc);
+								put3(py, O3(c_hi) + acc);
 							}
 						}
 					}
@@ -1222,6 +1296,7 @@ struct mm_solver {
 	// staged stage kernel: used when the rows are 16-byte aligned; grid and shared memory per stage
 	bool st_tma = false;
 	int st_tm = -1;                  // term set the staged kernel is specialised for (-1: run time)
+	bool st_pat = false;             // staged kernels compiled for the Dormand-Prince stage patterns
 	int st_resident = 0;             // resident blocks of k_stage on this solver's device
 	int st_grid[MAXS] = {};
 	size_t st_smem[MAXS] = {};
@@ -1470,6 +1545,11 @@ mm_status stage_tma_prepare(mm_solver *s)
 	const void *fn = s->st_tm == TM_SLAB   ? (const void *)k_stage_tma<T, COMP, S, TM_SLAB>
 	                 : s->st_tm == TM_FILM ? (const void *)k_stage_tma<T, COMP, S, TM_FILM>
 	                                       : (const void *)k_stage_tma<T, COMP, S, TM_RUNTIME>;
+	if constexpr (S <= 6) {
+		if (s->st_pat)
+			fn = s->st_tm == TM_SLAB ? (const void *)k_stage_tma<T, COMP, S, TM_SLAB, dp54_pattern(S, COMP)>
+			                         : (const void *)k_stage_tma<T, COMP, S, TM_FILM, dp54_pattern(S, COMP)>;
+	}
 	MM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - 2 * 256 * (int)sizeof(T)));
 	int per_sm = 0;
 	MM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, ST_CONS + 32, smem));
@@ -1527,6 +1607,24 @@ mm_status stage_tma_setup(mm_solver *s, std::integer_sequence<int, S...>)
 	s->st_tm = s->cfg.terms == TM_SLAB ? TM_SLAB : s->cfg.terms == TM_FILM ? TM_FILM : TM_RUNTIME;
 	if (const char *gen = std::getenv("MMB200_STAGE_GENERIC"))  // the run-time term set (comparison tests)
 		if (gen[0] == '1') s->st_tm = TM_RUNTIME;
+	// the Dormand-Prince stage patterns (the fixed term sets include demag), unless
+	// MMB200_STAGE_PATTERN=0; every stage's pattern must equal its coefficients' own
+	s->st_pat = (s->st_tm == TM_SLAB || s->st_tm == TM_FILM) && s->cfg.tableau == MM_RK_DP54 && s->tab.s == 7;
+	if (const char *pe = std::getenv("MMB200_STAGE_PATTERN"))
+		if (pe[0] == '0') s->st_pat = false;
+	for (int i = 0; i < s->tab.s && s->st_pat; ++i) {
+		// the pattern, and the operand layout the consumers derive from it, must equal the
+		// coefficients' own (the producer and the shared-memory size follow the coefficients)
+		const StageCoef sc = stage_coef(s->tab, i, COMP);
+		const int pat = dp54_pattern(i, COMP);
+		int kop[MAXS], hd, hi, lo;
+		const int nops = stage_ops(sc, i, COMP, true, kop, hd, hi, lo);
+		const bool out = pat_bit(pat, 7) ? pat_bit(pat, 9) : pat_bit(pat, 8);
+		bool same = pattern_of(sc, i) == pat && pat_nops(pat, COMP, true) == nops && hd == 0 &&
+		            hi == (out ? 1 : -1) && lo == (out && COMP ? 2 : -1);
+		for (int l = 0; l < MAXS; ++l) same = same && (l < PAT_KBITS ? pat_kop(pat, COMP, true, l) == kop[l] : kop[l] < 0);
+		if (!same) s->st_pat = false;
+	}
 	mm_status r = stage_tma_maps<T>(s);
 	((r = (r == MM_OK && S < s->tab.s) ? stage_tma_prepare<T, COMP, S>(s) : r), ...);
 	if (r != MM_OK) {
@@ -1547,6 +1645,18 @@ void stage_tma_launch(const mm_solver *s, const CellArgs<T> &a, const StageCoef 
 	(void)yhi;
 	(void)ylo;
 	const int tx = (c.nx + ST_X - 1) / ST_X, ty = (c.ny + ST_Y - 1) / ST_Y;
+	if constexpr (S <= 6) {
+		if (s->st_pat && s->st_tm == TM_SLAB) {
+			k_stage_tma<T, COMP, S, TM_SLAB, dp54_pattern(S, COMP)><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+			    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
+			return;
+		}
+		if (s->st_pat && s->st_tm == TM_FILM) {
+			k_stage_tma<T, COMP, S, TM_FILM, dp54_pattern(S, COMP)><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
+			    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
+			return;
+		}
+	}
 	if (s->st_tm == TM_SLAB)
 		k_stage_tma<T, COMP, S, TM_SLAB><<<s->st_grid[S], ST_CONS + 32, s->st_smem[S], st>>>(
 		    maps, a, sc, kt, yout, (T *)s->ynew_lo, ds, tx, ty);
@@ -2185,6 +2295,7 @@ MM_API mm_status mm_solver_stats_get(mm_solver *s, mm_solver_stats *out, void *s
 	out->last_error = sqrt(s->hst->max_err2);
 	out->last_max_dmdt = sqrt(s->hst->max_k02);
 	out->not_finite = s->not_finite;
+	out->stage_kernel = !s->st_tma ? 0 : s->st_tm == TM_RUNTIME ? 1 : s->st_pat ? 3 : 2;
 	return MM_OK;
 }
 
@@ -2443,6 +2554,8 @@ struct mm_batch {
 		mm_solver *s = nullptr;  // nullptr: free slot
 		mm::BSlot *dev = nullptr;
 		double t_end = 0.0;
+		bool stopped = false;    // seen stopped by a run-flag check: left out of rebuilt rounds
+		long long start_round = 0;  // the batch round in which the instance's first attempt runs
 	};
 	std::vector<Slot> slots;
 	std::vector<int> members;                     // slot index of each member of the built rounds
@@ -2456,8 +2569,12 @@ struct mm_batch {
 	size_t slots_h_cap = 0;
 	cudaStream_t gs = nullptr;
 	cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-	cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // [0] with k_0 evaluation, [1] without
-	int launches_per_round[2] = {0, 0};
+	// [0] round with k_0 evaluations, [1] without, [2] FP32 rebase phase
+	cudaGraphExec_t gexec[3] = {nullptr, nullptr, nullptr};
+	int launches_per_round[3] = {0, 0, 0};
+	long long rounds_total = 0;  // rounds run since creation (an instance's attempt count is the
+	                             // number of rounds since its start_round)
+	unsigned rebase_mask = 0;    // FP32: start rounds of the members, mod BATCH_REBASE
 };
 
 namespace mm {
@@ -2467,7 +2584,7 @@ void drop_rounds(mm_batch *b)
 {
 	for (auto &g : b->gexec)
 		if (g) cudaGraphExecDestroy(g);
-	b->gexec[0] = b->gexec[1] = nullptr;
+	b->gexec[0] = b->gexec[1] = b->gexec[2] = nullptr;
 	conv_group_destroy(b->conv);
 	b->conv = nullptr;
 	cudaFree(b->desc);
@@ -2534,16 +2651,6 @@ mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 	constexpr bool COMP = sizeof(T) == 4;
 	const Tableau tb = make_tableau(MM_RK_DP54);
 	const BDesc<T> *d = (const BDesc<T> *)b->desc;
-	if constexpr (COMP) {
-		// instances flagged for a rebase: base state, then its field (convolution output 1, gated
-		// by the rebase flag), then its exchange part
-		const BDesc<float> *df = (const BDesc<float> *)b->desc;
-		k_rebase_grp<<<b->n_cell3, 256, 0, st>>>(df, b->cell3_items);
-		MM_TRY(after_launch("k_rebase_grp"));
-		MM_TRY(conv_group_execute(b->conv, 0, 2, st, 1));
-		k_base_grp<<<b->n_cell, 256, 0, st>>>(df, b->cell_items);
-		MM_TRY(after_launch("k_base_grp"));
-	}
 	if (with_k0) {
 		StageCoef sc{};
 		sc.stage = 0;
@@ -2587,6 +2694,19 @@ mm_status batch_round(mm_batch *b, bool with_k0, cudaStream_t st)
 	return MM_OK;
 }
 
+// FP32 rebase phase, replayed before the rounds in which some member is due (the flag of each
+// instance decides whether it takes part): base state, then its field (convolution output 1,
+// gated by the rebase flag), then its exchange part.
+mm_status batch_rebase(mm_batch *b, cudaStream_t st)
+{
+	const BDesc<float> *df = (const BDesc<float> *)b->desc;
+	k_rebase_grp<<<b->n_cell3, 256, 0, st>>>(df, b->cell3_items);
+	MM_TRY(after_launch("k_rebase_grp"));
+	MM_TRY(conv_group_execute(b->conv, 0, 2, st, 1));
+	k_base_grp<<<b->n_cell, 256, 0, st>>>(df, b->cell_items);
+	return after_launch("k_base_grp");
+}
+
 template <typename T, bool COMP, int... S>
 mm_status stage_grp_attrs(std::integer_sequence<int, S...>)
 {
@@ -2611,7 +2731,7 @@ mm_status batch_graph(mm_batch *b, int v)
 	cudaGraph_t g = nullptr;
 	const uint64_t l0 = launch_counter().load();
 	MM_CUDA(cudaStreamBeginCapture(b->gs, cudaStreamCaptureModeThreadLocal));
-	const mm_status r = batch_round<T>(b, v == 0, b->gs);
+	const mm_status r = v == 2 ? batch_rebase(b, b->gs) : batch_round<T>(b, v == 0, b->gs);
 	const cudaError_t e = cudaStreamEndCapture(b->gs, &g);
 	if (r != MM_OK) {
 		if (g) cudaGraphDestroy(g);
@@ -2636,7 +2756,7 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 	std::vector<int2> si, c3, c1;
 	for (int k = 0; k < (int)b->slots.size(); ++k) {
 		const mm_batch::Slot &sl = b->slots[k];
-		if (!sl.s) continue;
+		if (!sl.s || sl.stopped) continue;
 		mm_solver *s = sl.s;
 		const int i = (int)b->members.size();
 		b->members.push_back(k);
@@ -2685,6 +2805,10 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 	MM_TRY((stage_grp_attrs<T, sizeof(T) == 4>(std::make_integer_sequence<int, 7>())));
 	MM_TRY(batch_graph<T>(b, 0));
 	MM_TRY(batch_graph<T>(b, 1));
+	if (sizeof(T) == 4) MM_TRY(batch_graph<T>(b, 2));
+	// residues (mod BATCH_REBASE) of the members' start rounds: the rounds that need the rebase phase
+	b->rebase_mask = 0;
+	for (int k : b->members) b->rebase_mask |= 1u << (b->slots[k].start_round % BATCH_REBASE);
 	return MM_OK;
 }
 
@@ -2857,6 +2981,12 @@ MM_API mm_status mm_batch_set_M(mm_batch *b, int slot, const double *M_device, v
 	cudaStream_t st = as_stream(stream);
 	MM_CUDA(cudaStreamSynchronize(b->gs));
 	MM_TRY(mm_solver_set_M(sl->s, M_device, stream));
+	if (sl->stopped) {  // left out of the rounds since it stopped: back in
+		sl->stopped = false;
+		b->dirty = true;
+	}
+	sl->start_round = b->rounds_total;  // its first attempt runs in the next round
+	b->rebase_mask |= 1u << (sl->start_round % BATCH_REBASE);
 	k_slot_start<<<1, 1, 0, st>>>(sl->s->dst, sl->dev, b->cfg.h0, sl->t_end);
 	MM_TRY(after_launch("k_slot_start"));
 	MM_CUDA(cudaStreamSynchronize(st));
@@ -2886,12 +3016,17 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 {
 	if (!b || max_rounds < 0 || check_interval < 1) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_relax: invalid argument");
 	cudaStream_t st = as_stream(stream);
-	if (b->dirty) {
-		std::lock_guard<std::mutex> lock(capture_mutex());
-		MM_TRY(b->prec == MM_F64 ? build_rounds<double>(b, st) : build_rounds<float>(b, st));
-	}
 	long long done = 0;
-	if (!b->members.empty()) {
+	// Rounds replay the graphs of the current members.  When a run-flag check finds half of them
+	// stopped, the rounds are rebuilt over the running ones (fewer work items and launches per
+	// round; an instance's arithmetic does not depend on the members around it).
+	for (bool compact = true; compact && done < max_rounds;) {
+		compact = false;
+		if (b->dirty) {
+			std::lock_guard<std::mutex> lock(capture_mutex());
+			MM_TRY(b->prec == MM_F64 ? build_rounds<double>(b, st) : build_rounds<float>(b, st));
+		}
+		if (b->members.empty()) break;
 		const size_t cnt = b->members.size();
 		if (b->slots_h_cap < cnt) {
 			cudaFreeHost(b->slots_h);
@@ -2902,19 +3037,32 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 		MM_CUDA(cudaEventRecord(b->ev_in, st));
 		MM_CUDA(cudaStreamWaitEvent(b->gs, b->ev_in, 0));
 		while (done < max_rounds) {
+			if (b->gexec[2] && (b->rebase_mask >> (b->rounds_total % BATCH_REBASE) & 1u)) {
+				MM_CUDA(cudaGraphLaunch(b->gexec[2], b->gs));
+				launch_counter().fetch_add(b->launches_per_round[2]);
+			}
 			const int v = b->any_need_k0 ? 0 : 1;
 			MM_CUDA(cudaGraphLaunch(b->gexec[v], b->gs));
 			launch_counter().fetch_add(b->launches_per_round[v]);
 			b->any_need_k0 = false;
 			++done;
+			++b->rounds_total;
 			if (done % check_interval == 0 || done == max_rounds) {
 				for (size_t i = 0; i < cnt; ++i)
 					MM_CUDA(cudaMemcpyAsync(&b->slots_h[i], b->slots[b->members[i]].dev, sizeof(BSlot),
 					                        cudaMemcpyDeviceToHost, b->gs));
 				MM_CUDA(cudaStreamSynchronize(b->gs));
-				int left = 0;
-				for (size_t i = 0; i < cnt; ++i) left += b->slots_h[i].active;
+				size_t left = 0;
+				for (size_t i = 0; i < cnt; ++i) {
+					left += b->slots_h[i].active ? 1 : 0;
+					if (!b->slots_h[i].active) b->slots[b->members[i]].stopped = true;
+				}
 				if (!left) break;
+				if (2 * left <= cnt && cnt > 1) {
+					b->dirty = true;
+					compact = true;
+					break;
+				}
 			}
 		}
 		MM_CUDA(cudaEventRecord(b->ev_out, b->gs));

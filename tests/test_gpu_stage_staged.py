@@ -27,14 +27,14 @@ def grains(sv, rng, count):
     return mats
 
 
-def run(sv, monkeypatch, dims, prec, regions, mats, terms, M, staged, grid_cap, steps=3):
+def run(sv, monkeypatch, dims, prec, regions, mats, terms, M, staged, grid_cap, steps=3, H_ext=(5e3, 0, 1e4)):
     monkeypatch.setenv("MMB200_STAGE_TMA", "1" if staged else "0")
     if grid_cap:
         monkeypatch.setenv("MMB200_STAGE_GRID", str(grid_cap))
     else:
         monkeypatch.delenv("MMB200_STAGE_GRID", raising=False)
     s = sv.Solver(sv.RectangularMesh(dims, (2e-9, 2e-9, 2e-9)), mats, regions=regions, terms=terms, precision=prec,
-                  evolver="dp54", eps_abs=1e-4, eps_rel=1e-4, H_ext=(5e3, 0, 1e4))
+                  evolver="dp54", eps_abs=1e-4, eps_rel=1e-4, H_ext=H_ext)
     s.M = M
     for _ in range(steps):
         s.step()
@@ -75,3 +75,31 @@ def test_staged_stage_follows_plain_stage(sv, monkeypatch, prec, dims, with_regi
     scale = float(m0.abs().max())
     tol = 1e-12 if prec == "f64" else 1e-6
     assert float((m1 - m0).abs().max()) / scale < tol
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("granular", [False, True])
+def test_stage_patterns_follow_the_runtime_stage(sv, monkeypatch, prec, granular):
+    # the staged kernels compiled for the Dormand-Prince stage patterns (the granular slab's and
+    # the film's term sets) against the same kernels reading the stage structure at run time
+    rng = np.random.default_rng(41 + granular)
+    dims = (128, 24, 5) if granular else (64, 16, 8)
+    n = int(np.prod(dims))
+    if granular:
+        mats = grains(sv, rng, 6)
+        reg = rng.integers(1, len(mats), size=n).astype(np.uint8)
+        reg[rng.random(n) < 0.05] = 0
+        terms = ("demag", "exchange", "uniaxial", "zhangli")
+    else:
+        mats = [sv.Material(Ms=8e5, A=1.3e-11, alpha=0.5)]
+        reg = None
+        terms = ("demag", "exchange")
+    M = unit_random(rng, n) * 1e6
+    monkeypatch.setenv("MMB200_STAGE_PATTERN", "1")
+    m1, st1 = run(sv, monkeypatch, dims, prec, reg, mats, terms, M, True, 5, steps=4, H_ext=(0, 0, 0))
+    monkeypatch.setenv("MMB200_STAGE_PATTERN", "0")
+    m0, st0 = run(sv, monkeypatch, dims, prec, reg, mats, terms, M, True, 5, steps=4, H_ext=(0, 0, 0))
+    assert st1["stage_kernel"] == 3 and st0["stage_kernel"] == 2
+    assert st1["steps"] == st0["steps"] and st1["rejected"] == st0["rejected"]
+    scale = float(m0.abs().max())
+    assert float((m1 - m0).abs().max()) / scale < (1e-14 if prec == "f64" else 1e-7)

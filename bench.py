@@ -483,7 +483,7 @@ def run_batch(args):
         res = b.results()
         d = sum(1 for x in res if x["status"] == 1)
         if d // 16 != done // 16:
-            progress.append([round(ms * 1e-3, 2), d])
+            progress.append([round(ms * 1e-3, 2), d, rounds])
         done = d
         if done + sum(1 for x in res if x["status"] == 2) == len(insts):
             break
@@ -506,7 +506,7 @@ def run_batch(args):
     value = len(finished) / (ms * 1e-3) if ms > 0 else 0.0
     line = {
         "metric": "batched relax solves/s", "value": value, "unit": "solves/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (compensated state; f64 step control)",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (deviation form: base state + deviation; f64 step control)",
         "data": "synthetic (seeded sizes, masks, materials, initial m)",
         "config": {"workload": f"{len(insts)} uneven instances, nx,ny in [16,256], nz in {{1,2,4}}, 4 nm cells, "
                                "elliptical masks, relaxed to max |m x H|/Ms < 1e-4, dp54",
@@ -514,7 +514,7 @@ def run_batch(args):
                    "device_time_budget_s": args.batch_budget,
                    "all_finished": len(finished) == len(insts), "launches_per_round": [first, later]},
         "device_ms": ms, "ms_per_round": ms / max(rounds, 1), "gpu_launches": launches,
-        "relaxed_vs_device_s": progress,
+        "relaxed_vs_device_s": progress, "relaxed_vs_device_s_fields": "device s, relaxed, rounds",
         "accepted_steps": sum(x["steps"] for x in res),
         "cell_rhs_evals_per_s": evals / (ms * 1e-3) if ms > 0 else 0.0,
         "fp64_one_at_a_time": {"solves_per_s": fp64_rate, "instances_solved": done64, "instances_timed": len(idx),
@@ -578,8 +578,10 @@ def run_serve(args):
     points, fp64_cache = [], {}
     for rate in rates:
         reqs = serve_requests(args.serve_requests, rate, SERVE_SEED)
+        caps = None if args.serve_max_live == "none" else [int(v) for v in args.serve_max_live.split(",")]
         srv = Server(memory_budget=int(args.serve_memory_gb * (1 << 30)), precision="f32", eps_abs=1e-3,
-                     eps_rel=1e-4, max_torque=SERVE_RELAX_TORQUE, check_every_nth_step=1, rounds_per_tick=16)
+                     eps_rel=1e-4, max_torque=SERVE_RELAX_TORQUE, check_every_nth_step=1, rounds_per_tick=16,
+                     max_live=caps)
         st = srv.run(reqs, deadline=args.serve_budget)
         srv.close()
         lat = [c.latency for c in st.completed] or [float("nan")]
@@ -620,11 +622,12 @@ def run_serve(args):
         print(json.dumps({"point": pt}), flush=True)
     line = {
         "metric": "served solves/s and p50/p99 latency", "value": points[-1]["solves_per_s"], "unit": "solves/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (compensated state; f64 step control)",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (deviation form: base state + deviation; f64 step control)",
         "data": "synthetic (seeded Poisson arrivals, sizes, masks, materials, pulses, initial m)",
         "config": {"workload": "relax (max |m x H|/Ms < 1e-3) and switching (1 ns, 100 ps pulse rise, 10-100 mT) "
                                "requests, sizes as the batched relaxations + 5% at 1024x1024x4",
-                   "memory_budget_gb": args.serve_memory_gb, "deadline_s": args.serve_budget},
+                   "memory_budget_gb": args.serve_memory_gb, "deadline_s": args.serve_budget,
+                   "max_live_per_class": args.serve_max_live, "requests_per_rate": args.serve_requests},
         "points": points,
     }
     print(json.dumps(line), flush=True)
@@ -687,6 +690,8 @@ def main():
                     help="requests per rate (enough to keep the server busy for the whole deadline)")
     ap.add_argument("--serve-rates", default="50,2000")
     ap.add_argument("--serve-memory-gb", type=float, default=100.0)
+    ap.add_argument("--serve-max-live", default="32,16,2",
+                    help="requests each size class runs at once (<=128k cells, <=1M, larger), or none")
     ap.add_argument("--serve-budget", type=float, default=90.0, help="seconds per arrival rate")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--batch-rounds", type=int, default=2000000)

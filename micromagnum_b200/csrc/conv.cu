@@ -1620,6 +1620,7 @@ ConvPlan::~ConvPlan()
 	cudaFree(tw_y);
 	cudaFree(tw_z);
 	cudaFree(tensor);
+	cudaFree(tensor_kx);
 	cudaFree(spec);
 	cudaFree(err);
 }
@@ -2049,7 +2050,6 @@ struct ConvGroup {
 	bool maps_ok = false;         // every member's maps exist (variant 3 possible)
 	int *err = nullptr;           // set when a staged pass gave up waiting
 	bool one_output = false;      // some member has no second output
-	std::vector<void *> owned;    // kx-major tensors of the fused members
 	// the lists of one phase (independent members) run side by side on these streams
 	static constexpr int POOL = 8;
 	cudaStream_t pool[POOL] = {};
@@ -2059,7 +2059,6 @@ struct ConvGroup {
 		cudaFree(desc);
 		cudaFree(maps);
 		cudaFree(err);
-		for (void *q : owned) cudaFree(q);
 		for (auto &l : lists) cudaFree(l.items);
 		for (auto &q : pool)
 			if (q) cudaStreamDestroy(q);
@@ -2396,7 +2395,7 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 	std::vector<GDesc<T>> h(count);
 	std::map<std::pair<int, int>, std::vector<int>> lists;  // (pass, length) -> members
 	for (int i = 0; i < count; ++i) {
-		const ConvPlan *p = m[i].plan;
+		ConvPlan *p = m[i].plan;
 		if (!p || p->prec != g->prec || p->is2d || !p->fast_x || !p->fast_y || !p->reg_z)
 			return fail(MM_ERR_UNSUPPORTED, "conv group: every member needs power-of-two 3-D padding with a register z pass");
 		if (2 * p->nx > p->px || 2 * p->ny > p->py || 2 * p->nz > p->pz)
@@ -2418,14 +2417,16 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 		lists[{0, p->px}].push_back(i);
 		if (yz_tb<T>(p) > 0) {
 			lists[{6, p->py * 64 + p->pz}].push_back(i);  // y, z and the multiply in one pass
-			// the fused pass reads the tensor by (kx, kz, ky) with its six components together
-			T *tt = nullptr;
-			const size_t ne = (size_t)6 * p->hx * p->qy * p->qz;
-			MM_CUDA(cudaMalloc(&tt, ne * sizeof(T)));
-			g->owned.push_back(tt);
-			k_tensor_kx<T><<<(unsigned)((ne + 255) / 256), 256, 0, st>>>((const T *)p->tensor, tt, p->hx, p->qy, p->qz);
-			MM_CUDA(cudaGetLastError());
-			d.tensor_t = tt;
+			// the fused pass reads the tensor by (kx, kz, ky) with its six components together;
+			// the plan keeps that copy, so regrouping (members joining or leaving) allocates nothing
+			if (!p->tensor_kx) {
+				const size_t ne = (size_t)6 * p->hx * p->qy * p->qz;
+				MM_CUDA(cudaMalloc(&p->tensor_kx, ne * sizeof(T)));
+				k_tensor_kx<T><<<(unsigned)((ne + 255) / 256), 256, 0, st>>>((const T *)p->tensor, (T *)p->tensor_kx,
+				                                                               p->hx, p->qy, p->qz);
+				MM_CUDA(cudaGetLastError());
+			}
+			d.tensor_t = (const T *)p->tensor_kx;
 		} else {
 			lists[{1, p->py}].push_back(i);
 			lists[{2, p->pz}].push_back(i);

@@ -37,6 +37,8 @@ struct ConvPlan {
 	FftRadices rx{}, ry{}, rz{};
 	void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;  // cplx<T> twiddle tables
 	void *tensor = nullptr;         // reduced real tensor spectrum, T[6][qz][qy][hx]
+	void *tensor_kx = nullptr;      // the same, kx-major T[hx][qz][qy][6] (made by the first grouped
+	                                // convolution whose fused y+z pass takes this plan)
 	void *spec = nullptr;           // cplx<T>[3][nz][py][lx]
 	// launch geometry
 	int lp_x = 1;                   // complex lines (= 2 real rows) per CTA in the x passes

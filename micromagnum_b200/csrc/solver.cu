@@ -506,7 +506,8 @@ __device__ __forceinline__ bool cell_rhs_delta(const CellArgs<T> &a, const T *__
 // DELTA (the FP32 batched form, with COMP): y_in, the combination and y_out are deviations from
 // the base state yhi (ylo: the step's own deviation D_n), hb the base field (cell_rhs_delta), and
 // the last stage writes the deviation of y_{n+1} into y_out alone (y_out_lo is not written).
-template <typename T, bool COMP, int S, bool TORQUE, bool DELTA = false>
+// PAT: the stage's structure at compile time (as in k_stage_tma), PAT_RUNTIME: from sc.
+template <typename T, bool COMP, int S, bool TORQUE, bool DELTA = false, int PAT = PAT_RUNTIME>
 __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__restrict__ msr, const StageCoef &sc,
                                            const T *__restrict__ y_in, const T *__restrict__ Hd,
                                            const T *__restrict__ yhi, const T *__restrict__ ylo, T *const *K,
@@ -515,6 +516,11 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
                                            T &e2, T &k02, T &tq2, T *pre, const T *__restrict__ hb = nullptr)
 {
 	static_assert(!DELTA || COMP, "the deviation form is the compensated FP32 form's");
+	constexpr bool CT = PAT != PAT_RUNTIME;
+	const bool s_last = CT ? pat_bit(PAT, 7) : sc.last != 0;
+	const bool s_wnext = CT ? pat_bit(PAT, 8) : sc.write_next != 0;
+	const bool s_wnew = CT ? pat_bit(PAT, 9) : sc.write_new != 0;
+	const bool s_rk0 = CT ? pat_bit(PAT, 10) : sc.reduce_k0 != 0;
 	const size_t n = (size_t)a.nx * a.ny * a.nz;
 	const double h = st->h;
 	const int tx = tile % tiles_x, rest = tile / tiles_x;
@@ -528,10 +534,10 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 	size_t idx[STAGE_CPT];
 	bool in[STAGE_CPT];
 	// which operands the combination needs (uniform over the block)
-	const bool out = sc.last ? sc.write_new : sc.write_next;
+	const bool out = s_last ? s_wnew : s_wnext;
 	bool needk[MAXS];
 #pragma unroll
-	for (int l = 0; l < MAXS; ++l) needk[l] = stage_needs_k(sc, S, l);
+	for (int l = 0; l < MAXS; ++l) needk[l] = CT ? (l < PAT_KBITS && pat_bit(PAT, l)) : stage_needs_k(sc, S, l);
 #pragma unroll
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		const int x = tx * (blockDim.x * STAGE_CPT) + threadIdx.x + u * blockDim.x;
@@ -578,19 +584,19 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 	for (int u = 0; u < STAGE_CPT; ++u) {
 		if (!in[u]) continue;
 		const size_t i = idx[u];
-		if (!sc.last) {
-			if (sc.write_next) {
+		if (!s_last) {
+			if (s_wnext) {
 				V3<T> acc = COMP ? pre3(u, 3) : pre3(u, 0);
 #pragma unroll
 				for (int l = 0; l < S; ++l) {
 					const T f = (T)(h * sc.bn[l]);
-					if (f != T(0)) acc = acc + f * pre3(u, 6 + 3 * l);
+					if (CT ? pat_bit(PAT, 11 + l) : f != T(0)) acc = acc + f * pre3(u, 6 + 3 * l);
 				}
 				acc = acc + (T)(h * sc.bn[S]) * ki[u];
 				if (COMP && !DELTA) acc = pre3(u, 0) + acc;
 				store3(y_out, i, n, acc);
 			}
-			if (sc.reduce_k0) {
+			if (s_rk0) {
 				const V3<T> k0 = S == 0 ? ki[u] : pre3(u, 6);
 				k02 = max(k02, dot(k0, k0));
 			}
@@ -601,13 +607,15 @@ __device__ __forceinline__ void stage_tile(const CellArgs<T> &a, const T *__rest
 			for (int l = 0; l <= S; ++l) {
 				const T fe = (T)(h * sc.ec[l]);
 				const T fc = (T)(h * sc.bn[l]);
-				if (fe == T(0) && (!sc.write_new || fc == T(0))) continue;
+				if (CT ? (!pat_bit(PAT, 18 + l) && (!s_wnew || !pat_bit(PAT, 11 + l)))
+				       : (fe == T(0) && (!s_wnew || fc == T(0))))
+					continue;
 				const V3<T> kl = l == S ? ki[u] : pre3(u, 6 + 3 * l);
 				err = err + fe * kl;
-				if (sc.write_new) acc = acc + fc * kl;
+				if (s_wnew) acc = acc + fc * kl;
 			}
 			e2 = nan_max(e2, dot(err, err));
-			if (sc.write_new) {
+			if (s_wnew) {
 				if (DELTA) {
 					store3(y_out, i, n, pre3(u, 3) + acc);  // deviation of y_{n+1} from the base state
 				} else if (COMP) {
@@ -693,10 +701,11 @@ struct StTmaGeom {
 };
 
 // Whether a box takes the staged stage kernel: rows of y_in (and of the region ids) start on
-// 16-byte boundaries.
-inline bool stage_tma_fits(int nx, size_t esize, bool regions)
+// 16-byte boundaries, and every element index of a 3N vector fits 32 bits (the consumers address
+// their stores with 32-bit offsets).
+inline bool stage_tma_fits(int nx, size_t esize, bool regions, size_t ncells)
 {
-	return (nx * esize) % 16 == 0 && (!regions || nx % 16 == 0);
+	return (nx * esize) % 16 == 0 && (!regions || nx % 16 == 0) && 3 * ncells < (size_t)1 << 31;
 }
 
 template <typename T, bool COMP, int S, int TM, int PAT = PAT_RUNTIME>
@@ -860,7 +869,7 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 				const int ly = ly0 + u * (ST_Y / ST_CPT), hr = ly + 1;
 				const int x = x0 + lx, yy = y0 + ly;
 				if (x < nx && yy < ny) {
-					const size_t i = ((size_t)z * ny + yy) * nx + x;
+					const uint32_t i = ((uint32_t)z * ny + yy) * nx + x, n32 = (uint32_t)n;
 					// this cell in the ring slots of planes z-1, z, z+1 (component stride YC) and in
 					// the operand buffer (operand stride OS, component stride OC); 32-bit offsets
 					constexpr int YC = ST_YH * ST_XH, OC = ST_Y * ST_X, OS = 3 * OC;
@@ -908,8 +917,8 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 					T *const pk = kS + i, *const py = y_out + i;
 					auto put3 = [&](T *p, V3<T> v) {
 						p[0] = v.x;
-						p[n] = v.y;
-						p[2 * n] = v.z;
+						p[n32] = v.y;
+						p[2 * n32] = v.z;
 					};
 					if (!s_last) {
 						if (s_wnext) {
@@ -1602,7 +1611,7 @@ mm_status stage_tma_setup(mm_solver *s, std::integer_sequence<int, S...>)
 	const char *env = std::getenv("MMB200_STAGE_TMA");
 	// the staged kernel's halo boxes do not wrap around: periodic meshes take the per-thread kernel
 	const bool periodic = s->cfg.pbc[0] || s->cfg.pbc[1] || s->cfg.pbc[2];
-	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr) && !(env && env[0] == '0') && !periodic;
+	s->st_tma = stage_tma_fits(s->cfg.nx, sizeof(T), s->reg != nullptr, s->n) && !(env && env[0] == '0') && !periodic;
 	if (!s->st_tma) return MM_OK;
 	s->st_tm = s->cfg.terms == TM_SLAB ? TM_SLAB : s->cfg.terms == TM_FILM ? TM_FILM : TM_RUNTIME;
 	if (const char *gen = std::getenv("MMB200_STAGE_GENERIC"))  // the run-time term set (comparison tests)
@@ -2349,11 +2358,11 @@ constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage
 constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
 // FP32 batches (deviation form, cell_rhs_delta): attempts between rebases of an instance.  The
 // stage inputs' rounding grows with the deviation accumulated since the last rebase.
-constexpr int BATCH_REBASE = 8;
+constexpr int BATCH_REBASE = 16;
 
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
 // K0: the k_0 evaluation of instances that need it (others skip it).
-template <typename T, bool COMP, int S, bool TORQUE>
+template <typename T, bool COMP, int S, bool TORQUE, int PAT>
 __global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
     k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items)
 {
@@ -2371,11 +2380,11 @@ __global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
 	T *const *K = g.kt->k;  // read per use (cached), not held in registers
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
 	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
-		stage_tile<T, COMP, S, TORQUE, COMP>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds,
+		stage_tile<T, COMP, S, TORQUE, COMP, PAT>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds,
 		                                     it.y + k, g.tiles_x, g.tiles_y, e2, k02, tq2,
 		                                     reinterpret_cast<T *>(stage_pre), g.hb);
-	if (sc.last) block_max_to(&g.ds->max_err2, e2);
-	if (sc.reduce_k0) block_max_to(&g.ds->max_k02, k02);
+	if (pat_bit(PAT, 7)) block_max_to(&g.ds->max_err2, e2);
+	if (pat_bit(PAT, 10)) block_max_to(&g.ds->max_k02, k02);
 	if (TORQUE) block_max_to(&g.ds->max_tq2, tq2);
 }
 
@@ -2613,21 +2622,26 @@ void free_batch(mm_batch *b)
 	delete b;
 }
 
+// The batch always runs the Dormand-Prince tableau: its stage kernels are compiled for the dp54
+// stage patterns (checked against the coefficients at capture).
 template <typename T, bool COMP, int S>
 void launch_stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, cudaStream_t st)
 {
 	const BDesc<T> *d = (const BDesc<T> *)b->desc;
+	constexpr int PAT = dp54_pattern(S, COMP);
 	if (sc.last)
-		k_stage_grp<T, COMP, S, true><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
-		                                                                               b->stage_items);
+		k_stage_grp<T, COMP, S, true, PAT><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
+		                                                                                    b->stage_items);
 	else
-		k_stage_grp<T, COMP, S, false><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
-		                                                                                b->stage_items);
+		k_stage_grp<T, COMP, S, false, PAT><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
+		                                                                                     b->stage_items);
 }
 
 template <typename T, bool COMP>
 mm_status stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, cudaStream_t st)
 {
+	if (sc.stage < 0 || sc.stage > 6 || pattern_of(sc, sc.stage) != dp54_pattern(sc.stage, COMP))
+		return fail(MM_ERR_INVALID_ARGUMENT, "batch: stage coefficients differ from the Dormand-Prince stage patterns");
 	switch (sc.stage) {
 	case 0: launch_stage_grp<T, COMP, 0>(b, sc, in, out, st); break;
 	case 1: launch_stage_grp<T, COMP, 1>(b, sc, in, out, st); break;
@@ -2712,11 +2726,11 @@ mm_status stage_grp_attrs(std::integer_sequence<int, S...>)
 {
 	const int bytes = (int)stage_smem<T>();
 	cudaError_t e = cudaSuccess;
-	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, false>,
+	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, false, dp54_pattern(S, COMP)>,
 	                                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
 	                       : e),
 	 ...);
-	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, true>,
+	((e = e == cudaSuccess ? cudaFuncSetAttribute(k_stage_grp<T, COMP, S, true, dp54_pattern(S, COMP)>,
 	                                              cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)
 	                       : e),
 	 ...);

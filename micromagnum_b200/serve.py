@@ -69,8 +69,9 @@ class ServeStats:
 class _Class:
     """One size class: a batch, its queue of arrived requests and its running requests."""
 
-    def __init__(self, batch: Batch):
+    def __init__(self, batch: Batch, max_live: Optional[int] = None):
         self.batch = batch
+        self.max_live = max_live
         self.queue = deque()
         self.live = {}  # slot -> (request, resident bytes, admitted)
 
@@ -78,18 +79,25 @@ class _Class:
 class Server:
     def __init__(self, memory_budget: int, precision: str = "f32", eps_abs: float = 1e-3, eps_rel: float = 1e-4,
                  max_torque: float = 1e-4, check_every_nth_step: int = 1, rounds_per_tick: int = 8,
-                 keep_results=False, class_bounds: Sequence[int] = (1 << 17, 1 << 20)):
+                 keep_results=False, class_bounds: Sequence[int] = (1 << 17, 1 << 20),
+                 max_live: Optional[Sequence[int]] = None):
         """class_bounds: upper cell counts of the size classes (a last class takes the rest).
         keep_results: False, True (final M as a (3, N) array) or "omf" (final M as the bytes of an
-        OMF binary-8 file, the wire format requests may also use for M0)."""
+        OMF binary-8 file, the wire format requests may also use for M0).
+        max_live: the most requests each class runs at once (None: as many as memory allows).
+        Under overload, running every admitted request at once shares the device among all of
+        them and finishes none early; a bound serves them in arrival order, a batch at a time."""
         self.budget = int(memory_budget)
         self.precision = precision
         self.rounds_per_tick = int(rounds_per_tick)
         self.keep_results = keep_results
         self.bounds = list(class_bounds)
+        self.max_live = list(max_live) if max_live is not None else [None] * (len(self.bounds) + 1)
+        if len(self.max_live) != len(self.bounds) + 1:
+            raise ValueError("max_live needs one bound per size class")
         self.classes = [_Class(Batch([], precision=precision, eps_abs=eps_abs, eps_rel=eps_rel,
-                                     max_torque=max_torque, check_every_nth_step=check_every_nth_step))
-                        for _ in range(len(self.bounds) + 1)]
+                                     max_torque=max_torque, check_every_nth_step=check_every_nth_step), cap)
+                        for cap in self.max_live]
 
     def _class_of(self, req: Request) -> _Class:
         n = req.instance.n
@@ -118,7 +126,7 @@ class Server:
                 admitted = False
                 while True:  # admit in arrival order while memory allows
                     with lock:
-                        if not cl.queue:
+                        if not cl.queue or (cl.max_live is not None and len(cl.live) >= cl.max_live):
                             break
                         req = cl.queue[0]
                         res, trans = req.instance.device_bytes(self.precision)

@@ -144,3 +144,16 @@ def test_budget_is_shared_by_all_size_classes(fake):
     srv.close()
     assert len(st.completed) == len(reqs) and st.unfinished == 0
     assert st.peak_resident <= budget
+
+
+def test_max_live_bounds_each_class(fake):
+    # plenty of memory, at most two requests of the class at once; the others wait in arrival order
+    reqs = make_requests(7, (32, 32, 1), need=lambda i: 6 + 2 * (i % 3))
+    srv = serve.Server(memory_budget=1 << 34, rounds_per_tick=2, max_live=(2, 4, 1))
+    st = srv.run(reqs)
+    srv.close()
+    assert len(st.completed) == len(reqs) and fake.live_max <= 2
+    adm = sorted(st.completed, key=lambda c: c.admitted)
+    assert [c.id for c in adm] == list(range(len(reqs)))
+    with pytest.raises(ValueError):
+        serve.Server(memory_budget=1 << 34, max_live=(2, 4))

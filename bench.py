@@ -470,6 +470,18 @@ def run_batch(args):
     for i, M in enumerate(M0):
         b.set_M(i, M)
     torch.cuda.synchronize()
+    if args.batch_profile > 0:
+        # profiling hook: 64 rounds, then the given number of rounds between cudaProfilerStart and
+        # cudaProfilerStop (ncu --profile-from-start off), every instance still running
+        b.relax(max_rounds=64, check_interval=64)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        b.relax(max_rounds=args.batch_profile, check_interval=args.batch_profile)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profiled_rounds": args.batch_profile, "launches_per_round": b.launches_per_round()}))
+        b.close()
+        return
     ms, rounds, done, progress = 0.0, 0, 0, []
     l0 = _lib.launches()
     while rounds < args.batch_rounds and ms * 1e-3 < args.batch_budget:
@@ -696,6 +708,8 @@ def main():
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)
     ap.add_argument("--batch-rounds", type=int, default=2000000)
     ap.add_argument("--batch-budget", type=float, default=900.0, help="device seconds for the batched rounds")
+    ap.add_argument("--batch-profile", type=int, default=0,
+                    help="profiling hook: run this many rounds inside cudaProfilerStart/Stop and exit")
     ap.add_argument("--batch-sample", type=int, default=16,
                     help="instances (a seeded sample) solved one at a time in FP64 for the ratio")
     ap.add_argument("--precision", choices=["f32", "f64"], default="f32",

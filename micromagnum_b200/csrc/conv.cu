@@ -1890,7 +1890,10 @@ __global__ void k_tensor_kx(const T *__restrict__ src, T *__restrict__ dst, int 
 	}
 }
 
-template <int PY, int PZ, class C>
+// NARROW: one kx column per CTA (a small group, such as the tail of a batch, then spreads over more
+// SMs); each line's transforms and each (ky, column)'s multiply are the same operations either
+// way, so the results do not depend on the choice.
+template <int PY, int PZ, class C, bool NARROW = false>
 struct YZGeom {
 	static constexpr int NZ = PZ / 2;  // planes a member of this group can have (nz <= pz/2)
 	static constexpr int R = ct_radix(PY), TPL = PY / R;
@@ -1899,7 +1902,7 @@ struct YZGeom {
 	{
 		return (tb > 1 && (size_t)3 * NZ * tb * line_bytes * 33 / 32 > 104 * 1024) ? tb_for(tb / 2) : tb;
 	}
-	static constexpr int TB = tb_for(8);
+	static constexpr int TB = NARROW ? 1 : tb_for(8);
 	static constexpr int L = 3 * NZ * TB;
 	static constexpr int g_for(int g) { return ((L / g) * TPL > 512 && L % (2 * g) == 0) ? g_for(g * 2) : g; }
 	static constexpr int G = g_for(1);
@@ -1910,12 +1913,12 @@ struct YZGeom {
 	static constexpr bool fits = SMEM <= 227 * 1024 && THREADS >= 32 && THREADS <= 1024 && L % G == 0;
 };
 
-template <typename T, int PY, int PZ>
-__global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>>::THREADS)
+template <typename T, int PY, int PZ, bool NARROW = false>
+__global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>, NARROW>::THREADS)
     k_yz_grp(const GDesc<T> *__restrict__ d, const int2 *__restrict__ items, int gate)
 {
 	using C = cplx<T>;
-	using G = YZGeom<PY, PZ, C>;
+	using G = YZGeom<PY, PZ, C, NARROW>;
 	constexpr int TB = G::TB, LG = G::LG, NZ = G::NZ, H = PZ / 2;
 	using SI = SmCols<PY, LG>;
 	const int2 it = items[blockIdx.x];
@@ -2145,8 +2148,13 @@ int group_threads(int pass, int len, int v)
 	if (pass == 2) return v == 0 ? ZR_THREADS : 0;
 	if (pass == 6) {
 		int t = 0;
-		if (v == 0)
-			with_yz(len, [&](auto pyc, auto pzc) { t = YZGeom<decltype(pyc)::value, decltype(pzc)::value, C>::THREADS; });
+		with_yz(len, [&](auto pyc, auto pzc) {
+			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
+			using G0 = YZGeom<PY, PZ, C>;
+			using G1 = YZGeom<PY, PZ, C, true>;
+			if (v == 0 && G0::fits) t = G0::THREADS;
+			if (v == 1 && G1::fits && G0::fits && G0::TB > 1) t = G1::THREADS;
+		});
 		return t;
 	}
 	if (v == 3) {
@@ -2173,7 +2181,7 @@ int group_blocks(const ConvPlan *p, int pass, int len, int v)
 		return ((3 * p->ny * p->nz + 1) / 2 + lpb - 1) / lpb;
 	}
 	if (pass == 6) {
-		const int tb = yz_tb<T>(p);
+		const int tb = v == 1 ? 1 : yz_tb<T>(p);
 		return (p->hx + tb - 1) / tb;
 	}
 	if (pass == 1 || pass == 3) {
@@ -2190,7 +2198,10 @@ size_t group_smem_bytes(int pass, int len, int v)
 	size_t r = 0;
 	if (pass == 2) return zr_smem<T>(len);
 	if (pass == 6) {
-		with_yz(len, [&](auto pyc, auto pzc) { r = YZGeom<decltype(pyc)::value, decltype(pzc)::value, C>::SMEM; });
+		with_yz(len, [&](auto pyc, auto pzc) {
+			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
+			r = v == 1 ? YZGeom<PY, PZ, C, true>::SMEM : YZGeom<PY, PZ, C>::SMEM;
+		});
 		return r;
 	}
 	if (v == 3) {
@@ -2220,7 +2231,11 @@ mm_status group_smem(int pass, int len, int v)
 	if (pass == 6) {
 		with_yz(len, [&](auto pyc, auto pzc) {
 			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
-			if constexpr (YZGeom<PY, PZ, C>::fits) r = set_smem<T>((const void *)k_yz_grp<T, PY, PZ>, sm);
+			if (v == 1) {
+				if constexpr (YZGeom<PY, PZ, C, true>::fits) r = set_smem<T>((const void *)k_yz_grp<T, PY, PZ, true>, sm);
+			} else {
+				if constexpr (YZGeom<PY, PZ, C>::fits) r = set_smem<T>((const void *)k_yz_grp<T, PY, PZ>, sm);
+			}
 		});
 		return r;
 	}
@@ -2266,7 +2281,12 @@ void group_launch_v(const ConvGroup *g, int pass, int len, int v, const int2 *it
 		with_yz(len, [&](auto pyc, auto pzc) {
 			constexpr int PY = decltype(pyc)::value, PZ = decltype(pzc)::value;
 			using G = YZGeom<PY, PZ, C>;
-			if constexpr (G::fits) k_yz_grp<T, PY, PZ><<<n, G::THREADS, sm, st>>>(d, items, gate);
+			using GN = YZGeom<PY, PZ, C, true>;
+			if (v == 1) {
+				if constexpr (GN::fits) k_yz_grp<T, PY, PZ, true><<<n, GN::THREADS, sm, st>>>(d, items, gate);
+			} else {
+				if constexpr (G::fits) k_yz_grp<T, PY, PZ><<<n, G::THREADS, sm, st>>>(d, items, gate);
+			}
 		});
 		return;
 	}
@@ -2477,7 +2497,13 @@ mm_status group_create(ConvGroup *g, const ConvGroupMember *m, int count, cudaSt
 			v = (f >= 0 && f < GRP_VARIANTS && group_threads<T>(pass, len, f)) ? f : 0;
 			known = true;
 		}
-		if (pass == 6) known = true, v = 0;  // one variant
+		if (pass == 6) {
+			// the narrow tiles when the default ones would not fill the device twice over
+			int blocks = 0;
+			for (int i : kv.second) blocks += group_blocks<T>(m[i].plan, 6, len, 0);
+			known = true;
+			v = blocks < 2 * num_sms() && group_threads<T>(6, len, 1) > 0 ? 1 : 0;
+		}
 		if (!known) {
 			MM_TRY(group_tune<T>(g, m, kv.second, pass, len, st, &v));
 			std::lock_guard<std::mutex> lock(g_tune_mu);

@@ -2354,7 +2354,7 @@ struct BDesc {
 	int n, tiles_x, tiles_y, ntiles;
 };
 
-constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage kernel
+constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage kernel (1 for small batches)
 constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
 // FP32 batches (deviation form, cell_rhs_delta): attempts between rebases of an instance.  The
 // stage inputs' rounding grows with the deviation accumulated since the last rebase.
@@ -2364,7 +2364,7 @@ constexpr int BATCH_REBASE = 16;
 // K0: the k_0 evaluation of instances that need it (others skip it).
 template <typename T, bool COMP, int S, bool TORQUE, int PAT>
 __global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
-    k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items)
+    k_stage_grp(const BDesc<T> *__restrict__ d, StageCoef sc, int in, int out, const int2 *__restrict__ items, int tpi)
 {
 	const int2 it = items[blockIdx.x];
 	const BDesc<T> &g = d[it.x];
@@ -2379,7 +2379,7 @@ __global__ void __launch_bounds__(256, TORQUE ? 2 : stage_min_blocks<T>())
 	const T *y_in = in == 0 ? (COMP ? g.m_lo : g.m) : g.ys[in - 1];
 	T *const *K = g.kt->k;  // read per use (cached), not held in registers
 	T e2 = T(0), k02 = T(0), tq2 = T(0);
-	for (int k = 0; k < BATCH_TILES && it.y + k < g.ntiles; ++k)
+	for (int k = 0; k < tpi && it.y + k < g.ntiles; ++k)
 		stage_tile<T, COMP, S, TORQUE, COMP, PAT>(a, msr, sc, y_in, g.hd, g.m, g.m_lo, K, g.ys[out], g.ynew_lo, g.ds,
 		                                     it.y + k, g.tiles_x, g.tiles_y, e2, k02, tq2,
 		                                     reinterpret_cast<T *>(stage_pre), g.hb);
@@ -2573,6 +2573,7 @@ struct mm_batch {
 	mm::ConvGroup *conv = nullptr;
 	void *desc = nullptr;                         // BDesc<T>[members]
 	int2 *stage_items = nullptr, *cell3_items = nullptr, *cell_items = nullptr;
+	int tiles_per_item = 4;                       // stage tiles per item of the grouped stage kernel
 	int n_stage = 0, n_cell3 = 0, n_cell = 0;
 	mm::BSlot *slots_h = nullptr;                 // pinned copies for result queries
 	size_t slots_h_cap = 0;
@@ -2631,10 +2632,12 @@ void launch_stage_grp(const mm_batch *b, const StageCoef &sc, int in, int out, c
 	constexpr int PAT = dp54_pattern(S, COMP);
 	if (sc.last)
 		k_stage_grp<T, COMP, S, true, PAT><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
-		                                                                                    b->stage_items);
+		                                                                                    b->stage_items,
+		                                                                                    b->tiles_per_item);
 	else
 		k_stage_grp<T, COMP, S, false, PAT><<<b->n_stage, dim3(32, 8, 1), stage_smem<T>(), st>>>(d, sc, in, out,
-		                                                                                     b->stage_items);
+		                                                                                     b->stage_items,
+		                                                                                     b->tiles_per_item);
 }
 
 template <typename T, bool COMP>
@@ -2768,6 +2771,18 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 	std::vector<BDesc<T>> h;
 	std::vector<ConvGroupMember> mem;
 	std::vector<int2> si, c3, c1;
+	// stage tiles per work item: four while the tiles fill the device twice over, else one (a
+	// small batch, such as the tail of a relaxation, then spreads over more SMs; per-cell
+	// arithmetic and the maxima do not depend on the grouping)
+	{
+		long long tiles = 0;
+		for (const mm_batch::Slot &sl : b->slots)
+			if (sl.s && !sl.stopped) {
+				const dim3 tg = stage_grid(sl.s->cfg);
+				tiles += (long long)tg.x * tg.y * tg.z;
+			}
+		b->tiles_per_item = tiles >= 2LL * BATCH_TILES * 3 * num_sms() ? BATCH_TILES : 1;
+	}
 	for (int k = 0; k < (int)b->slots.size(); ++k) {
 		const mm_batch::Slot &sl = b->slots[k];
 		if (!sl.s || sl.stopped) continue;
@@ -2793,7 +2808,7 @@ mm_status build_rounds(mm_batch *b, cudaStream_t st)
 		d.tiles_y = (int)tg.y;
 		d.ntiles = (int)(tg.x * tg.y * tg.z);
 		h.push_back(d);
-		for (int t = 0; t < d.ntiles; t += BATCH_TILES) si.push_back(make_int2(i, t));
+		for (int t = 0; t < d.ntiles; t += b->tiles_per_item) si.push_back(make_int2(i, t));
 		for (int c = 0; (size_t)c * BATCH_CHUNK < 3 * s->n; ++c) c3.push_back(make_int2(i, c));
 		for (int c = 0; (size_t)c * BATCH_CHUNK < s->n; ++c) c1.push_back(make_int2(i, c));
 		mem.push_back(ConvGroupMember{s->conv, {s->m, s->ys[0], s->ys[1], s->m_lo},

@@ -177,3 +177,24 @@ def test_fp32_batch_end_states_vs_fp64_oracle(bt, oracle_mod):
         print(f"{q.dims}: batch {r['steps']} steps, oracle {steps}; max |dm| {dm:.2e}, |d<m>| {davg:.2e}")
         assert abs(r["steps"] - steps) <= 0.1 * steps
         assert davg < 5e-5 and dm < 2e-4
+
+
+def test_fused_pass_tiles_do_not_change_results(bt):
+    # five members of one fused y+z length (py = 512, pz = 4) fill the device with the default
+    # tiles; alone, the member takes one kx column per CTA: the same arithmetic, bit for bit
+    rng = np.random.default_rng(14)
+    insts = make_instances(bt, rng, [(200, 210, 2), (190, 220, 2), (210, 200, 2), (230, 180, 2), (200, 200, 2)])
+    M0 = [initial(q, rng) for q in insts]
+    mix = bt.Batch(insts, precision="f32", eps_abs=1e-3, eps_rel=1e-4, max_torque=1e-9, check_every_nth_step=1)
+    for i, M in enumerate(M0):
+        mix.set_M(i, M)
+    mix.relax(max_rounds=40, check_interval=40)
+    alone = bt.Batch([insts[3]], precision="f32", eps_abs=1e-3, eps_rel=1e-4, max_torque=1e-9,
+                     check_every_nth_step=1)
+    alone.set_M(0, M0[3])
+    alone.relax(max_rounds=40, check_interval=40)
+    r_mix, r_alone = mix.results()[3], alone.results()[0]
+    assert r_mix["attempts"] == r_alone["attempts"] == 40 and r_mix["steps"] == r_alone["steps"]
+    assert torch.equal(mix.get_M(3), alone.get_M(0))
+    mix.close()
+    alone.close()

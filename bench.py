@@ -702,7 +702,7 @@ def main():
                     help="requests per rate (enough to keep the server busy for the whole deadline)")
     ap.add_argument("--serve-rates", default="50,2000")
     ap.add_argument("--serve-memory-gb", type=float, default=100.0)
-    ap.add_argument("--serve-max-live", default="32,16,2",
+    ap.add_argument("--serve-max-live", default="64,16,1",
                     help="requests each size class runs at once (<=128k cells, <=1M, larger), or none")
     ap.add_argument("--serve-budget", type=float, default=90.0, help="seconds per arrival rate")
     ap.add_argument("--batch-count", type=int, default=BATCH_COUNT)

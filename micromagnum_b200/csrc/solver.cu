@@ -234,12 +234,13 @@ __device__ __forceinline__ void cell_core(const CellArgs<T> &a, const DevMat<T> 
 		// fdm_zhangli_cpu.cpp:100-200: u = (j.grad)M from raw M = Ms m (no Ms masking),
 		// one-sided at the borders, zero along a dimension of size 1
 		const V3<T> Mc = scale_rn(ms, m);
+		// one-sided at either face (both faces at once along a dimension of size 1: zero), central
+		// inside, with the operands selected rather than branched on
 		auto grad = [&](int c, int dim, int lo, T inv1, T inv2) -> V3<T> {
-			if (dim <= 1) return v3<T>(0, 0, 0);
 			const V3<T> Ml = scale_rn(nms[lo], nb[lo]), Mr = scale_rn(nms[lo + 1], nb[lo + 1]);
-			if (c == 0) return inv1 * (Mr - Mc);
-			if (c == dim - 1) return inv1 * (Mc - Ml);
-			return inv2 * (Mr - Ml);
+			const bool at_lo = c == 0, at_hi = c == dim - 1;
+			const V3<T> A = at_lo ? Mc : Ml, B = at_hi ? Mc : Mr;
+			return (at_lo || at_hi ? inv1 : inv2) * (B - A);
 		};
 		V3<T> u = v3<T>(0, 0, 0);
 		if (M.j[0] != T(0)) u = u + M.j[0] * grad(x, a.nx, 0, a.idx1, a.idx2);
@@ -904,12 +905,14 @@ __global__ void __launch_bounds__(ST_CONS + 32, StTmaGeom<T>::MINB)
 						T nms[6];
 						// every neighbour read stays inside the staged planes (the halo past the grid
 						// reads as zero, a missing plane z -+ 1 is a stale ring slot), so the reads
-						// are unconditional and the neighbours outside the box are masked afterwards
+						// are unconditional and the neighbours outside the box are masked afterwards:
+						// their Ms always (the halo's region ids read as region 0), their m only
+						// along z (an x or y neighbour past the grid is the zero fill already)
 #pragma unroll
 						for (int q = 0; q < 6; ++q) {
 							const V3<T> v = Y3(yq[q], dq[q]);
 							const T ms_q = a.reg ? msr[rq[q][drq[q]]] : M.Ms;
-							nb[q] = has[q] ? v : v3<T>(0, 0, 0);
+							nb[q] = (q < 4 || has[q]) ? v : v3<T>(0, 0, 0);
 							nms[q] = has[q] ? ms_q : T(0);
 						}
 						cell_core<T, TM>(a, M, m, nb, nms, x, yy, z, hd, Hz, Heff, ki);

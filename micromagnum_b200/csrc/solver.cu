@@ -2361,7 +2361,7 @@ constexpr int BATCH_TILES = 4;     // stage tiles per block of the grouped stage
 constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-wise kernels
 // FP32 batches (deviation form, cell_rhs_delta): attempts between rebases of an instance.  The
 // stage inputs' rounding grows with the deviation accumulated since the last rebase.
-constexpr int BATCH_REBASE = 16;
+constexpr int BATCH_REBASE = 32;
 
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
 // K0: the k_0 evaluation of instances that need it (others skip it).
@@ -3090,7 +3090,7 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 					if (!b->slots_h[i].active) b->slots[b->members[i]].stopped = true;
 				}
 				if (!left) break;
-				if (2 * left <= cnt && cnt > 1) {
+				if (4 * left <= 3 * cnt && cnt > 1) {
 					b->dirty = true;
 					compact = true;
 					break;

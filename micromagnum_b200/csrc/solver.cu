@@ -2362,6 +2362,7 @@ constexpr int BATCH_CHUNK = 4096;  // elements per block of the grouped element-
 // FP32 batches (deviation form, cell_rhs_delta): attempts between rebases of an instance.  The
 // stage inputs' rounding grows with the deviation accumulated since the last rebase.
 constexpr int BATCH_REBASE = 32;
+static_assert(BATCH_REBASE <= 32, "the due rounds are kept as a 32-bit mask of residues");
 
 // Grouped fused stage: block = (instance, first tile); in = 0: the state m, 1/2: ys[0]/ys[1].
 // K0: the k_0 evaluation of instances that need it (others skip it).
@@ -3049,8 +3050,8 @@ MM_API mm_status mm_batch_relax(mm_batch *b, long long max_rounds, int check_int
 	if (!b || max_rounds < 0 || check_interval < 1) return fail(MM_ERR_INVALID_ARGUMENT, "mm_batch_relax: invalid argument");
 	cudaStream_t st = as_stream(stream);
 	long long done = 0;
-	// Rounds replay the graphs of the current members.  When a run-flag check finds half of them
-	// stopped, the rounds are rebuilt over the running ones (fewer work items and launches per
+	// Rounds replay the graphs of the current members.  When a run-flag check finds a quarter of
+	// them stopped, the rounds are rebuilt over the running ones (fewer work items and launches per
 	// round; an instance's arithmetic does not depend on the members around it).
 	for (bool compact = true; compact && done < max_rounds;) {
 		compact = false;

@@ -1863,6 +1863,9 @@ __device__ __forceinline__ void cp_async_c(C *dst, const C *src)
 		asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all_c() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit_c() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group_c() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // Fused y and z passes for small members (the autotuner-free path of the grouped convolution):
 // one CTA takes a tile of TB x-frequency columns of one member and keeps all of its y-z data in
@@ -1909,7 +1912,12 @@ struct YZGeom {
 	static constexpr int LG = L / G;
 	static constexpr int THREADS = LG * TPL;
 	static constexpr size_t GROUP_ELEMS = SmCols<PY, LG>::SIZE;
-	static constexpr size_t SMEM = (size_t)G * GROUP_ELEMS * sizeof(C);
+	static constexpr size_t DATA = ((size_t)G * GROUP_ELEMS * sizeof(C) + 15) / 16 * 16;
+	// behind the y-z data: the tile's reduced tensor entries, kx-major [TB][PZ/2+1][PY/2+1][6],
+	// copied in while the forward y transforms run
+	static constexpr int QY = PY / 2 + 1, QZ = PZ / 2 + 1;
+	static constexpr size_t TENS = (size_t)TB * QZ * QY * 6 * (sizeof(C) / 2);
+	static constexpr size_t SMEM = DATA + TENS;
 	static constexpr bool fits = SMEM <= 227 * 1024 && THREADS >= 32 && THREADS <= 1024 && L % G == 0;
 };
 
@@ -1958,7 +1966,18 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>, NARROW>::THREADS)
 			}
 		}
 	}
-	cp_async_wait_all_c();
+	cp_async_commit_c();
+	// the tile's tensor entries: one contiguous run of the kx-major tensor (columns kx < hx)
+	using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+	T2 *tsm = reinterpret_cast<T2 *>(smem_raw + G::DATA);
+	{
+		const int cols = hx - kx0 < TB ? hx - kx0 : TB;
+		const int pairs = cols * G::QZ * G::QY * 3;
+		const C *src = reinterpret_cast<const C *>(g.tensor_t + (size_t)kx0 * G::QZ * G::QY * 6);
+		for (int e = tid; e < pairs; e += G::THREADS) cp_async_c(reinterpret_cast<C *>(tsm) + e, src + e);
+	}
+	cp_async_commit_c();
+	cp_async_wait_group_c<1>();  // the y-z data (the tensor may still be arriving)
 	__syncthreads();
 	// forward y transforms in place (rows ny.. are the zero padding)
 	for (int grp = 0; grp < G::G; ++grp) {
@@ -1968,6 +1987,7 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>, NARROW>::THREADS)
 		auto st = [&](int ll, int k, C v) { sm[SI::at(ll, k)] = v; };
 		cta_fft_h0<T, PY, G::R, LG, SI, true>(sm, g.tw_y, line, j0, ld, st);  // rows ny <= PY/2 .. are zero
 	}
+	cp_async_wait_group_c<0>();
 	__syncthreads();
 	// z transforms, tensor multiply, inverse z transforms: one thread per (ky, column)
 	for (int item = tid; item < PY * TB; item += G::THREADS) {
@@ -1985,12 +2005,11 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>, NARROW>::THREADS)
 		const int kyr = fy ? PY - ky : ky;
 		const T sy = fy ? T(-1) : T(1);
 		// kz and PZ - kz share the tensor entries (sign of the z-odd components flipped): each
-		// reduced entry is loaded once
-		using T2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+		// reduced entry is read once
 #pragma unroll
 		for (int kzr = 0; kzr <= H; ++kzr) {
-			// the six components of entry (kx, kzr, kyr), contiguous (8- or 16-byte aligned pairs)
-			const T2 *t = reinterpret_cast<const T2 *>(g.tensor_t + (((size_t)kx * g.qz + kzr) * g.qy + kyr) * 6);
+			// the six components of entry (kx, kzr, kyr), contiguous pairs in shared memory
+			const T2 *t = tsm + ((col * G::QZ + kzr) * G::QY + kyr) * 3;
 			const T2 t0 = t[0], t1 = t[1], t2 = t[2];
 			const T nxx = t0.x, nxy = t0.y, nxz = t1.x, nyy = t1.y, nyz = t2.x, nzz = t2.y;
 #pragma unroll

@@ -1911,7 +1911,7 @@ struct YZGeom {
 	static constexpr int G = g_for(1);
 	static constexpr int LG = L / G;
 	static constexpr int THREADS = LG * TPL;
-	static constexpr size_t GROUP_ELEMS = SmCols<PY, LG>::SIZE;
+	static constexpr size_t GROUP_ELEMS = SmCols<PY, LG, 4>::SIZE;
 	static constexpr size_t DATA = ((size_t)G * GROUP_ELEMS * sizeof(C) + 15) / 16 * 16;
 	// behind the y-z data: the tile's reduced tensor entries, kx-major [TB][PZ/2+1][PY/2+1][6],
 	// copied in while the forward y transforms run
@@ -1928,7 +1928,7 @@ __global__ void __launch_bounds__(YZGeom<PY, PZ, cplx<T>, NARROW>::THREADS)
 	using C = cplx<T>;
 	using G = YZGeom<PY, PZ, C, NARROW>;
 	constexpr int TB = G::TB, LG = G::LG, NZ = G::NZ, H = PZ / 2;
-	using SI = SmCols<PY, LG>;
+	using SI = SmCols<PY, LG, 4>;
 	const int2 it = items[blockIdx.x];
 	if (member_skips(d[it.x].flags, gate)) return;
 	const GDesc<T> &g = d[it.x];

@@ -592,8 +592,8 @@ def run_serve(args):
         reqs = serve_requests(args.serve_requests, rate, SERVE_SEED)
         caps = None if args.serve_max_live == "none" else [int(v) for v in args.serve_max_live.split(",")]
         srv = Server(memory_budget=int(args.serve_memory_gb * (1 << 30)), precision="f32", eps_abs=1e-3,
-                     eps_rel=1e-4, max_torque=SERVE_RELAX_TORQUE, check_every_nth_step=1, rounds_per_tick=16,
-                     max_live=caps)
+                     eps_rel=1e-4, max_torque=SERVE_RELAX_TORQUE, check_every_nth_step=1,
+                     rounds_per_tick=args.serve_tick, max_live=caps)
         st = srv.run(reqs, deadline=args.serve_budget)
         srv.close()
         lat = [c.latency for c in st.completed] or [float("nan")]
@@ -639,7 +639,8 @@ def run_serve(args):
         "config": {"workload": "relax (max |m x H|/Ms < 1e-3) and switching (1 ns, 100 ps pulse rise, 10-100 mT) "
                                "requests, sizes as the batched relaxations + 5% at 1024x1024x4",
                    "memory_budget_gb": args.serve_memory_gb, "deadline_s": args.serve_budget,
-                   "max_live_per_class": args.serve_max_live, "requests_per_rate": args.serve_requests},
+                   "max_live_per_class": args.serve_max_live, "requests_per_rate": args.serve_requests,
+                   "rounds_per_tick": args.serve_tick},
         "points": points,
     }
     print(json.dumps(line), flush=True)
@@ -702,6 +703,7 @@ def main():
                     help="requests per rate (enough to keep the server busy for the whole deadline)")
     ap.add_argument("--serve-rates", default="50,2000")
     ap.add_argument("--serve-memory-gb", type=float, default=100.0)
+    ap.add_argument("--serve-tick", type=int, default=8, help="rounds per serving tick")
     ap.add_argument("--serve-max-live", default="64,16,1",
                     help="requests each size class runs at once (<=128k cells, <=1M, larger), or none")
     ap.add_argument("--serve-budget", type=float, default=90.0, help="seconds per arrival rate")

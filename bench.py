@@ -584,6 +584,26 @@ def serve_requests(count, rate, seed):
     return out
 
 
+def fifo_queue(reqs, makespan, solve):
+    """One-at-a-time service of `reqs` in arrival order within `makespan` seconds.  solve(r, cap)
+    returns (seconds, steps, finished) of request r's full solve, given up after `cap` seconds
+    (the time left in the window).  The queue stops where it passes the makespan.  Returns
+    (requests solved in the window, their latencies, solve seconds spent inside the window)."""
+    t_free, lat, done, spent = 0.0, [], 0, 0.0
+    for r in sorted(reqs, key=lambda r: r.arrival):
+        start = max(t_free, r.arrival)
+        if start >= makespan:
+            break
+        cap = makespan - start
+        sec, _, finished = solve(r, cap)
+        spent += min(sec, cap)
+        t_free = start + sec
+        if finished and t_free <= makespan:
+            lat.append(t_free - r.arrival)
+            done += 1
+    return done, lat, spent
+
+
 def run_serve(args):
     from micromagnum_b200.serve import Server
     rates = [float(v) for v in args.serve_rates.split(",")]
@@ -603,20 +623,14 @@ def run_serve(args):
         # server's makespan, and the queue stops where it passes the makespan (the solve in progress
         # there is cut at that point, so nothing after it is measured)
         done_ids = {c.id for c in st.completed}
-        t_free, lat64, done64, measured64 = 0.0, [], 0, 0.0
-        for r in sorted(reqs, key=lambda r: r.arrival):
-            start = max(t_free, r.arrival)
-            if start >= st.makespan:
-                break
-            cap = st.makespan - start
+
+        def solve64(r, cap):
             c = fp64_cache.get(r.id)
             if c is None or (not c[2] and c[0] < cap):
                 c = fp64_cache[r.id] = fp64_solve(r.instance, r.M0, max_torque=SERVE_RELAX_TORQUE, cap_s=cap)
-            measured64 += min(c[0], cap)
-            t_free = start + c[0]
-            if c[2] and t_free <= st.makespan:
-                lat64.append(t_free - r.arrival)
-                done64 += 1
+            return c
+
+        done64, lat64, measured64 = fifo_queue(reqs, st.makespan, solve64)
         pt = {
             "rate_per_s": rate, "requests": len(reqs), "completed": len(st.completed), "unfinished": st.unfinished,
             "solves_per_s": st.solves_per_s, "p50_s": float(np.percentile(lat, 50)),
